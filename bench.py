@@ -1,0 +1,298 @@
+"""Benchmark: cell-bin SSP-RK3 updates per second of the seamount-eddies workload on B200.
+
+Default workload: 1024^2 grid (5 km, periodic), 32 vertical levels for the Q-transform,
+32 log-spaced kappa x 36 directions, seeded seamount depth and eddy currents, FP32
+state with FP64 tables (the precision form). One step = one SSP-RK3 step over all
+1.21e9 cell-bins. `value` is device-timed with the state resident in HBM; `e2e` runs
+the same steps through the public API (set!, time_step!, a per-step total-action
+read, interior) with pinned host buffers. --impl reference times the reference's CPU
+path (the FP64 C++ restatement) on the host cores instead.
+
+python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--precision fp32|fp64]
+               [--size 1024]
+Under torchrun each rank advances its own copy of the workload (independent replicas).
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "ripple.jl_b200"))
+
+import numpy as np  # noqa: E402
+
+METRIC = "cell·bin RK3 updates/s on 1 B200, FP32/learned vs plain FP64, at stated rel-L2"
+UNIT = "cell·bin updates/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--size", type=int, default=1024)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock and throttle-reason samples every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p is not None:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self):
+        self.f.flush()
+        rows = []
+        try:
+            with open(self.f.name) as f:
+                for line in f:
+                    parts = [x.strip() for x in line.split(",")]
+                    if len(parts) >= 9:
+                        rows.append(parts)
+        finally:
+            os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        busy = [s for s in sm if mx and s > 0.5 * max(mx)] or sm
+        return {"sm_mhz": statistics.median(busy) if busy else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def algorithmic_bytes(w, precision):
+    """Per RK3 step: 8 state words per unit (N0->N1; N1,N0->N2; N2,N0->N3) + per stage the FP64
+    per-(i,j,kappa) tables (Ux, Uy, 4 gradients, and c_g when depth varies) amortised over phi."""
+    s = 4 if precision == "fp32" else 8
+    Nk, Np = w.spectral_grid.coordinate_size()
+    c_d = 0 if np.isscalar(w.depth) or type(w.depth).__name__ == "InfiniteDepth" else 1
+    tables = 3 * (6 + c_d) * 8 * (w.units // Np) if w.velocities is not None else 3 * c_d * 8 * (w.units // Np)
+    return 8 * s * w.units + tables
+
+
+def cpu_baseline(size_hint, steps=4):
+    """The oracle (FP64 C++ restatement of the reference CPU path, OpenMP) on a bounded sample."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from ripple_b200 import workloads
+    n = 128
+    w = workloads.seamount_eddies(N=n, Nz=32, Nk=32, Np=36, nsteps=steps)
+    o = oracle.Oracle(w)
+    o.step(w.N0, w.dt, 1)
+    t = time.perf_counter()
+    o.step(w.N0, w.dt, steps)
+    el = time.perf_counter() - t
+    return {"value": w.units * steps / el, "unit": UNIT, "cores": oracle.num_threads(), "kind": "port",
+            "sample": f"seamount_eddies at {n}^2 x 32 kappa x 36 phi (same physics, reduced grid), "
+                      f"{steps} RK3 steps FP64, {el:.1f} s"}
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from ripple_b200 import workloads
+    n = 96
+    w = workloads.seamount_eddies(N=n, Nz=32, Nk=32, Np=36, nsteps=1)
+    o = oracle.Oracle(w)
+    N = w.N0
+    for _ in range(args.warmup):
+        N, _ = o.step(N, w.dt, 1)
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        N, _ = o.step(N, w.dt, 1)
+    el = time.perf_counter() - t
+    value = w.units * args.steps / el
+    sample = (f"each step one FP64 SSP-RK3 step of seamount_eddies at {n}^2 x 32 kappa x 36 phi "
+              f"(1024^2 does not fit a bounded CPU sample); per-unit throughput")
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "impl": "reference",
+            "config": {"workload": "seamount_eddies", "grid": [n, n, 32], "spectral": [32, 36],
+                       "precision": "fp64", "path": "reference CPU path restated in C++ (oracle/), OpenMP"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": oracle.num_threads(), "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import ripple_b200 as rp
+    from ripple_b200 import _lib, workloads
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    w = workloads.seamount_eddies(N=args.size, Nz=32, Nk=32, Np=36, nsteps=args.steps, n0_dtype=np.float32)
+    m = w.model(args.precision, device=local_rank)
+    lib, h = m._lib, m.handle
+    torch_stream = torch.cuda.Stream(device=local_rank)
+    _lib.check(lib.rpl_set_stream(h, _lib.ctypes.c_void_p(torch_stream.cuda_stream)))
+    dt = w.dt
+
+    # warm-up
+    for _ in range(args.warmup):
+        _lib.check(lib.rpl_step_async(h, dt, 1))
+    _lib.check(lib.rpl_sync(h))
+    barrier()
+
+    # device-timed region: K steps, events around each stage launch on the launching stream
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clk:
+        barrier()
+        with torch.cuda.stream(torch_stream):
+            start.record(torch_stream)
+            for k in range(args.steps):
+                ev[k][0].record(torch_stream)
+                for s in (1, 2, 3):
+                    _lib.check(lib.rpl_stage_async(h, dt, s))
+                    ev[k][s].record(torch_stream)
+            end.record(torch_stream)
+        torch_stream.synchronize()
+        _lib.check(lib.rpl_sync(h))
+        barrier()
+    ms = start.elapsed_time(end)
+    stage_ms = [ev[k][s].elapsed_time(ev[k][s + 1]) for k in range(args.steps) for s in range(3)]
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    clocks = clk.summary()
+    value = world * w.units * args.steps / (ms / 1e3)
+
+    # roofline of the dominant kernel (the fused stage kernel: one launch per RK3 stage)
+    peak, peak_kind = peaks()
+    launch_ms = statistics.mean(stage_ms)
+    bytes_per_launch = algorithmic_bytes(w, args.precision) / 3.0
+    achieved = bytes_per_launch / (launch_ms / 1e3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "stage_traffic.json")
+    if os.path.exists(tp):
+        try:
+            traffic = json.load(open(tp)).get(f"{args.precision}_{args.size}")
+        except Exception:
+            traffic = None
+
+    # end to end through the public API with pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        host = torch.empty(w.units, dtype=torch.float32 if args.precision == "fp32" else torch.float64,
+                           pin_memory=True)
+        hv = host.numpy()
+        hv[:] = np.ravel(w.N0, order="F")
+        tot = np.zeros(1)
+        barrier()
+        t0 = time.perf_counter()
+        _lib.check(lib.rpl_set_action(h, _lib.ctypes.c_void_p(host.data_ptr()),
+                                      _lib.RPL_F32 if args.precision == "fp32" else _lib.RPL_F64, 0))
+        for _ in range(args.steps):
+            _lib.check(lib.rpl_step(h, dt, 1))
+            _lib.check(lib.rpl_diagnostics(h, None, None, None, None, _lib.dptr(tot)))
+        _lib.check(lib.rpl_get_action(h, _lib.ctypes.c_void_p(host.data_ptr()),
+                                      _lib.RPL_F32 if args.precision == "fp32" else _lib.RPL_F64, 0))
+        el = time.perf_counter() - t0
+        if dist is not None:
+            t = torch.tensor([el], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            el = float(t.item())
+        nbytes = host.numel() * host.element_size()
+        e2e = {"value": world * w.units * args.steps / el, "unit": UNIT,
+               "h2d_bytes_per_step": nbytes / args.steps, "d2h_bytes_per_step": (nbytes + 8 * args.steps) / args.steps,
+               "includes": "set! from pinned host, K x (time_step! + total_action read), interior to pinned host"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(args.size)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32" if args.precision == "fp32" else "f64",
+            "data": "synthetic (seeded seamount depth, eddy currents, JONSWAP-like N0)",
+            "config": {"workload": "seamount_eddies", "grid": [args.size, args.size, 32], "spectral": [32, 36],
+                       "precision": args.precision, "units_per_step": w.units, "dt": dt,
+                       "l2": "state (%.1f GB per buffer) larger than L2; no flush" % (w.units * (4 if args.precision == "fp32" else 8) / 1e9),
+                       "parallelism": f"{world} independent replicas" if world > 1 else "1 GPU"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": traffic, "peak_kind": peak_kind, "kernel": "stage_kernel",
+                         "launch_ms": launch_ms, "algorithmic_bytes_per_launch": bytes_per_launch},
+            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": 3 * args.steps, "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    m.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

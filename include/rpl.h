@@ -1,0 +1,185 @@
+/*
+ * rpl.h -- C-ABI of librpl.so, the B200 (sm_100a) implementation of Ripple.jl's
+ * time-step hot path: SSP-RK3 stages fused with WENO5 Doppler transport and
+ * spectral refraction, the Q-transform Doppler velocity, and the wind-input /
+ * whitecapping source terms.
+ *
+ * Plain C types only: pointers, sizes, scalars. One CUDA stream per handle; a
+ * handle is not thread-safe, different handles may be used from different
+ * threads. Every entry point returns an rpl_status; on failure
+ * rpl_last_error() returns a thread-local message. No entry point traps or
+ * aborts on bad input. Host arrays passed in are copied; the library never
+ * keeps a caller's pointer after the call returns.
+ *
+ * Array layout RPL_LAYOUT_XFAST: element (i,j,m,n) of an (Nx,Ny,Nk,Np) array at
+ * i + Nx*(j + Ny*(m + Nk*n)), i.e. the interior of the reference's ProductField
+ * flat_data (src/ProductFields/product_field.jl:65-82) without its halo and
+ * z slab. 2-D (Nx,Ny) and 3-D (Nx,Ny,Nz|Nk) arrays follow the same x-fastest rule.
+ *
+ * Reference interfaces each entry point replaces are cited per declaration
+ * (paths inside NumericalEarth/Ripple.jl).
+ */
+#ifndef RPL_H
+#define RPL_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RPL_ABI_VERSION 1
+
+typedef struct rpl_handle rpl_handle;
+
+typedef enum rpl_status {
+    RPL_OK = 0,
+    RPL_ERR_ARGUMENT = 1,     /* bad descriptor, size or pointer (reference: ArgumentError) */
+    RPL_ERR_DT = 2,           /* dt <= 0 or non-finite (time_step.jl:120) */
+    RPL_ERR_NONFINITE = 3,    /* non-finite input values */
+    RPL_ERR_CUDA = 4,         /* CUDA runtime error */
+    RPL_ERR_OOM = 5,          /* device allocation failed or would exceed the memory limit */
+    RPL_ERR_STATE = 6,        /* call out of order (e.g. refraction step before rpl_set_currents) */
+    RPL_ERR_UNSUPPORTED = 7,  /* configuration outside the B200 path (e.g. non-periodic x,y) */
+    RPL_ERR_DEVICE = 8        /* a kernel raised its error word (non-finite state produced) */
+} rpl_status;
+
+typedef enum rpl_precision { RPL_FP64 = 0, RPL_FP32 = 1 } rpl_precision;
+typedef enum rpl_dtype { RPL_F64 = 0, RPL_F32 = 1 } rpl_dtype;
+typedef enum rpl_layout { RPL_LAYOUT_XFAST = 0 } rpl_layout;
+
+typedef enum rpl_transport {
+    RPL_TRANSPORT_NONE = 0,        /* no transport (source-only columns) */
+    RPL_TRANSPORT_REFRACTION = 1,  /* wave_current_refraction.jl:74-151 (needs rpl_set_currents) */
+    RPL_TRANSPORT_INTRINSIC = 2    /* intrinsic_transport.jl:14-68 */
+} rpl_transport;
+
+typedef enum rpl_depth_kind {
+    RPL_DEPTH_INFINITE = 0,  /* deep water, cell-averaged c_g (transport.jl:61-70) */
+    RPL_DEPTH_CONSTANT = 1,  /* cell-centre finite-depth c_g (transport.jl:72-83) */
+    RPL_DEPTH_FIELD = 2      /* per-(i,j) depth, x fastest */
+} rpl_depth_kind;
+
+typedef enum rpl_wind_kind {
+    RPL_WIND_NONE = 0,
+    RPL_WIND_UNIFORM = 1,    /* scalar U10 and direction */
+    RPL_WIND_HOLLAND = 2,    /* HollandHurricaneWind + LinearStormTrack, evaluated on the device */
+    RPL_WIND_FIELD = 3       /* per-(i,j) U10 and direction from rpl_set_wind_field */
+} rpl_wind_kind;
+
+/* Model descriptor: the data SpectralWaveModel(grid, spectral_grid; depth, ...) carries
+ * (src/Models/spectral_wave_model.jl:155-211) restricted to this path. */
+typedef struct rpl_desc {
+    int32_t abi_version;        /* RPL_ABI_VERSION */
+    int32_t precision;          /* rpl_precision of the state and stencil arithmetic */
+    int32_t transport;          /* rpl_transport */
+    int32_t device;             /* CUDA device ordinal */
+    int64_t Nx, Ny, Nk, Np;     /* physical cells and (kappa, phi) bins */
+    double dx, dy;              /* first(xspacings(grid)), first(yspacings(grid)) */
+    const double* xnodes;       /* Nx cell centres (wind evaluation) */
+    const double* ynodes;       /* Ny cell centres */
+    int32_t periodic_x, periodic_y;  /* must both be 1 for any transport (tendencies.jl:43-50) */
+    const double* kappa;        /* Nk centres, strictly increasing, > 0 */
+    const double* kappa_faces;  /* Nk+1 faces */
+    const double* phi;          /* Np centres */
+    const double* phi_faces;    /* Np+1 faces */
+    int32_t depth_kind;         /* rpl_depth_kind: model depth for dispersion */
+    double depth_constant;
+    const double* depth_field;  /* Nx*Ny */
+    double gravity;             /* 9.81 in the reference */
+    int64_t memory_limit_bytes; /* 0: no limit; else creation fails with RPL_ERR_OOM above it */
+} rpl_desc;
+
+/* Source bundle: PrecomputedSources(wind_input=PressureCorrelationInput(...),
+ * dissipation=LocalSaturationDissipation(...)) (src/Physics/Packages/precomputed_sources.jl:179-191),
+ * or either term alone (stress_cap = 0 reproduces a bare PressureCorrelationInput). */
+typedef struct rpl_sources {
+    int32_t wind_kind;          /* rpl_wind_kind */
+    int32_t stress_cap;         /* 1: wave-supported stress cap (precomputed_sources.jl:282-326) */
+    int32_t drag_form;          /* 0: BulkWindDrag(:linear), 1: BulkWindDrag(:capped) (drag.jl:77-86) */
+    int32_t rotation;           /* Holland: +1 counterclockwise, -1 clockwise */
+    double wind_speed, wind_direction;           /* RPL_WIND_UNIFORM */
+    double vmax, rmax, radius, shape_parameter;  /* RPL_WIND_HOLLAND (winds.jl:200-229) */
+    double inflow_angle, background_x, background_y;
+    int64_t n_track;            /* 0: fixed centre (track_x[0], track_y[0]) */
+    const double* track_t;      /* LinearStormTrack times (winds.jl:115-152) */
+    const double* track_x;
+    const double* track_y;
+    /* PressureCorrelationInput parameters (pressure_correlation.jl:39-52) */
+    double beta_max, z_alpha, p_in, alpha0, rho_air, rho_water, von_karman, wind_gravity;
+    /* LocalSaturationDissipation parameters (local_saturation.jl:18-28) */
+    int32_t has_dissipation;
+    int32_t reserved;
+    double C_ds, B_r, ds_p, sigma_power, ds_gravity;
+} rpl_sources;
+
+/* Replaces SpectralWaveModel construction (spectral_wave_model.jl:155-211): validates the descriptor,
+ * allocates the device state (three state buffers, coefficient tables) and builds the c_g tables
+ * (transport.jl:111-139). The action starts at zero like WaveActionField (product_field.jl:310). */
+int rpl_create(const rpl_desc* desc, rpl_handle** out);
+int rpl_destroy(rpl_handle* h);
+
+/* Replaces build_coupling(PrescribedVelocities) + update_coupling! (lagrangian_velocities.jl:434-440,
+ * current_coupling.jl:127-138): Q-transform Doppler velocity U and dU/dkappa on the device
+ * (doppler_velocity.jl:45-82, q_kernel.jl:60-116) and their periodic gradients
+ * (wave_current_refraction.jl:7-39). u, v: (Nx,Ny,Nz) x fastest; z_faces: Nz+1 increasing;
+ * q_depth: column depth for the projection (grid depth for InfiniteDepth, lagrangian_velocities.jl:340-342). */
+int rpl_set_currents(rpl_handle* h, int64_t Nz, const double* z_faces,
+                     int32_t q_depth_kind, double q_depth_constant, const double* q_depth_field,
+                     const double* u, const double* v, double small_mu);
+/* Copies the cached coupling fields to the host (coupling.Ux/Uy/dUxdkappa/dUydkappa and
+ * coupling.Ux_x/Ux_y/Uy_x/Uy_y of current_coupling.jl:19-39); any pointer may be NULL. (Nx,Ny,Nk) each. */
+int rpl_get_coupling(rpl_handle* h, double* Ux, double* Uy, double* dUxdk, double* dUydk,
+                     double* Uxx, double* Uxy, double* Uyx, double* Uyy);
+
+/* Replaces the sources kwarg + prepare_sources (precomputed_sources.jl:386-394). */
+int rpl_set_sources(rpl_handle* h, const rpl_sources* s);
+/* Host-evaluated wind (any wind struct of src/Forcing/winds.jl) for RPL_WIND_FIELD: (Nx,Ny) arrays. */
+int rpl_set_wind_field(rpl_handle* h, const double* U10, const double* direction);
+
+/* Replaces set!(model, N=array) / set!(::ProductField, ::AbstractArray) (set.jl:20-30,44-48). */
+int rpl_set_action(rpl_handle* h, const void* N, int32_t dtype, int32_t layout);
+/* Replaces interior(model.action) (product_field.jl:232-235). */
+int rpl_get_action(rpl_handle* h, void* N, int32_t dtype, int32_t layout);
+/* Device-resident variants: N points to device memory on the handle's device (same layout). */
+int rpl_set_action_device(rpl_handle* h, const void* N, int32_t dtype, int32_t layout);
+int rpl_get_action_device(rpl_handle* h, void* N, int32_t dtype, int32_t layout);
+
+/* Clock (Oceananigans Clock of spectral_wave_model.jl:148): time and iteration. */
+int rpl_set_clock(rpl_handle* h, double time, int64_t iteration);
+int rpl_get_clock(rpl_handle* h, double* time, int64_t* iteration);
+
+/* Replaces time_step!(model, dt) with timestepper=:RK3 (time_step.jl:119-170), nsteps times.
+ * Returns after the stream has drained and the kernels' error word was checked. */
+int rpl_step(rpl_handle* h, double dt, int64_t nsteps);
+/* Same launches, no final synchronisation or error-word check (use rpl_sync). */
+int rpl_step_async(rpl_handle* h, double dt, int64_t nsteps);
+/* Launches exactly one RK3 stage (1, 2 or 3) of the step starting at the current clock; for
+ * per-kernel timing. Stage 3 advances the clock. */
+int rpl_stage_async(rpl_handle* h, double dt, int32_t stage);
+int rpl_sync(rpl_handle* h);
+/* Use the caller's CUDA stream (a cudaStream_t on the handle's device) instead of the handle's own. */
+int rpl_set_stream(rpl_handle* h, void* stream);
+
+/* Replaces compute_tendencies!(model) (tendencies.jl:18-41,82-101): G of the current action
+ * (transport plus sources) copied to the host in FP64. For testing. */
+int rpl_tendency(rpl_handle* h, double* G, int32_t layout);
+
+/* Replaces m0, significant_wave_height, root_mean_square_wavenumber, mean_direction
+ * (moments.jl:33-123, bulk_statistics.jl:9) as (Nx,Ny) fields and total_action (bulk_statistics.jl:87-91)
+ * as a scalar; FP64 with compensated sums on the device. Any pointer may be NULL. */
+int rpl_diagnostics(rpl_handle* h, double* m0, double* hs, double* krms, double* mean_dir,
+                    double* total_action);
+
+/* Device bytes held by the handle. */
+int rpl_device_bytes(rpl_handle* h, int64_t* bytes);
+/* Thread-local message of the last failing call on this thread ("" if none). */
+const char* rpl_last_error(void);
+/* ABI version the library was built with. */
+int rpl_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,122 @@
+/*
+ * ripple_oracle.h -- TEST INFRASTRUCTURE ONLY.
+ *
+ * CPU FP64 restatement of Ripple.jl's time-step path (NumericalEarth/Ripple.jl).
+ * It is the correctness oracle for the CUDA library and the timed CPU baseline.
+ * Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline / reference
+ * arm load it; the product path (librpl.so) never links, loads or calls it.
+ *
+ * Parity status: pinned against the reference's own known-answer tests
+ * (Q-transform integrals and Doppler sums, barotropic currents, WENO5 sinusoid
+ * transport, RK3 source column, Holland wind and storm track, bulk drag); the
+ * fused 4-D refraction kernel and multi-step RK3 trajectories have no golden
+ * vectors in the reference, so for those the restatement itself is the pin.
+ *
+ * Layout of every 4-D array: x fastest, i.e. element (i,j,m,n) at
+ * i + Nx*(j + Ny*(m + Nk*n)), the interior of the reference's
+ * ProductField flat_data (src/ProductFields/product_field.jl:65-82) without halo.
+ */
+#ifndef RIPPLE_ORACLE_H
+#define RIPPLE_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { ORA_TRANSPORT_NONE = 0, ORA_TRANSPORT_REFRACTION = 1, ORA_TRANSPORT_INTRINSIC = 2 };
+enum { ORA_WIND_NONE = 0, ORA_WIND_UNIFORM = 1, ORA_WIND_HOLLAND = 2, ORA_WIND_FIELD = 3 };
+
+typedef struct ora_holland {
+    double vmax, rmax, radius, shape_parameter, inflow_angle;
+    double background_x, background_y;
+    int32_t rotation;          /* +1 counterclockwise, -1 clockwise */
+    int32_t n_track;           /* 0: fixed centre (center_x[0], center_y[0]) */
+    const double* track_t;     /* n_track strictly increasing times */
+    const double* center_x;    /* n_track (or 1) centres */
+    const double* center_y;
+} ora_holland;
+
+typedef struct ora_model {
+    int64_t Nx, Ny, Nk, Np;
+    double dx, dy;                       /* first(xspacings), first(yspacings) */
+    const double* xnodes;                /* Nx cell centres */
+    const double* ynodes;                /* Ny cell centres */
+    const double* kappa;                 /* Nk centres */
+    const double* kappa_faces;           /* Nk+1 */
+    const double* phi;                   /* Np centres */
+    const double* phi_faces;             /* Np+1 */
+    const double* weights;               /* (Nk,Np) m fastest */
+    int32_t transport;
+    int32_t cg_per_cell;                 /* 0: cg tables (Nk,Np); 1: (Nx,Ny,Nk,Np) */
+    const double* cg_x;
+    const double* cg_y;
+    /* refraction inputs, (Nx,Ny,Nk) x fastest */
+    const double* Ux; const double* Uy;
+    const double* Uxx; const double* Uxy; const double* Uyx; const double* Uyy;
+    /* sources: PrecomputedSources(wind_input, dissipation) */
+    int32_t wind_kind;
+    double wind_speed, wind_direction;   /* ORA_WIND_UNIFORM */
+    ora_holland holland;                 /* ORA_WIND_HOLLAND */
+    const double* wind_U10;              /* ORA_WIND_FIELD: (Nx,Ny) */
+    const double* wind_theta;
+    double beta_max, z_alpha, p_in, alpha0, rho_air, rho_water, von_karman, gravity;
+    int32_t has_dissipation;
+    double C_ds, B_r, ds_p, sigma_power, ds_gravity;
+} ora_model;
+
+/* ---- Q kernel (src/Coupling/q_kernel.jl) ---- */
+double ora_q_value(double kappa, double z, double depth, double small_mu);
+double ora_q_cdf(double kappa, double z, double depth, double small_mu);
+double ora_q_cell_integral(double kappa, double z1, double z2, double depth, double small_mu);
+double ora_q_cdf_kappa_derivative(double kappa, double z, double depth, double small_mu);
+double ora_q_cell_integral_kappa_derivative(double kappa, double z1, double z2, double depth, double small_mu);
+double ora_q_cdf_kernel(double kappa, double z, double depth, double small_mu);
+double ora_q_cell_integral_kernel(double kappa, double z1, double z2, double depth, double small_mu);
+double ora_q_cell_integral_kappa_derivative_kernel(double kappa, double z1, double z2, double depth, double small_mu);
+
+/* ---- Doppler velocity and its gradients ---- */
+void ora_doppler_velocity(int64_t Nx, int64_t Ny, int64_t Nz, int64_t Nk,
+                          const double* u, const double* v,
+                          const double* depth_field, double depth_scalar,
+                          const double* kappa, const double* zfaces, double small_mu,
+                          int32_t derivative, double* Ux, double* Uy);
+void ora_current_gradients(int64_t Nx, int64_t Ny, int64_t Nk,
+                           const double* Ux, const double* Uy, double dx_inv, double dy_inv,
+                           double* Uxx, double* Uxy, double* Uyx, double* Uyy);
+
+/* ---- spectral grid and group velocity ---- */
+void ora_lower_bounded_faces(int64_t N, const double* centers, double lower, double* faces);
+void ora_uniform_periodic_faces(int64_t N, const double* centers, double* faces);
+void ora_polar_weights(int64_t Nk, int64_t Np, const double* kf, const double* pf, double* w);
+void ora_group_velocity_deep(int64_t Nk, int64_t Np, const double* kf, const double* pf,
+                             const double* w, double gravity, double* cg_x, double* cg_y);
+void ora_group_velocity_finite(int64_t Nx, int64_t Ny, int64_t Nk, int64_t Np,
+                               const double* kappa, const double* phi,
+                               const double* depth_field, double depth_scalar, double gravity,
+                               double* cg_x, double* cg_y);
+
+/* ---- winds and drag ---- */
+double ora_friction_velocity_linear(double U10);
+void ora_holland_velocity(const ora_holland* w, double x, double y, double t, double* vx, double* vy);
+void ora_storm_center(const ora_holland* w, double t, double* cx, double* cy);
+void ora_wind_fields(const ora_model* M, double t, double* U10, double* theta, double* ustar);
+
+/* ---- tendencies, sources, RK3 ---- */
+void ora_tendency(const ora_model* M, const double* N, double t, int32_t with_sources, double* G);
+void ora_stress_factor(const ora_model* M, const double* N, double t, double* factor);
+void ora_rk3_step(const ora_model* M, double* N, double dt, int64_t nsteps, double* t);
+
+/* ---- diagnostics (src/Diagnostics) ---- */
+void ora_diagnostics(const ora_model* M, const double* N,
+                     double* m0, double* hs, double* krms, double* mean_dir, double* total_action);
+
+int ora_num_threads(void);
+void ora_set_num_threads(int n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,109 @@
+// rpl_internal.h -- handle layout and kernel launchers shared by the librpl.so translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/rpl.h"
+
+namespace rpl {
+
+// Device-side view of the model handed to every stage kernel (by value).
+struct StageParams {
+    int64_t Nx, Ny, Nk, Np;
+    double dx_inv, dy_inv, dk_inv, dp_inv;  // 1/first spacing (wave_current_refraction.jl:200-203)
+    double dt;
+    double a, b;                            // stage combine: out = max(0, a*N0 + b*max(0, N + dt*G))
+    int stage;                              // 1, 2, 3
+    int transport;
+    int cg_per_cell;                        // 1: cg magnitude per (i,j,m) times direction table
+    // tables (FP64)
+    const double* kappa;                    // Nk
+    const double* phi;                      // Np
+    const double* weights;                  // (Nk,Np) spectral cell measures
+    const double* cosp;                     // Np
+    const double* sinp;                     // Np
+    const double* cg_x;                     // (Nk,Np) tables, or direction cosines when cg_per_cell
+    const double* cg_y;
+    const double* cg_mag;                   // (Nx,Ny,Nk) when cg_per_cell
+    const double* Ux;                       // (Nx,Ny,Nk)
+    const double* Uy;
+    const double* Uxx;
+    const double* Uxy;
+    const double* Uyx;
+    const double* Uyy;
+    // sources
+    int has_wind, stress_cap, has_diss;
+    const double* wind_U10;                 // (Nx,Ny)
+    const double* wind_theta;
+    const double* wind_ustar;
+    const double* stress_factor;            // (Nx,Ny)
+    double rho_ratio, beta_max, z_alpha, p_in, alpha0, von_karman, wind_g;
+    double C_ds, B_r, ds_p, sigma_power, ds_g;
+    unsigned int* err;                      // device error word
+};
+
+struct Handle {
+    rpl_desc desc{};
+    std::vector<double> xnodes, ynodes, kappa, kappa_faces, phi, phi_faces, depth_field, weights;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int precision = RPL_FP64;
+    size_t elem = 8;
+    int64_t units = 0, cells = 0;
+    // state: N (current), A, B (stage buffers)
+    void* N = nullptr;
+    void* A = nullptr;
+    void* B = nullptr;
+    // tables
+    double* d_kappa = nullptr;
+    double* d_phi = nullptr;
+    double* d_cos = nullptr;
+    double* d_sin = nullptr;
+    double* d_weights = nullptr;
+    double* d_cgx = nullptr;
+    double* d_cgy = nullptr;
+    double* d_cgmag = nullptr;
+    double* d_depth = nullptr;
+    double* d_coupling = nullptr;  // 8 arrays of (Nx,Ny,Nk): Ux Uy dUxdk dUydk Uxx Uxy Uyx Uyy
+    bool currents_set = false;
+    // sources
+    rpl_sources src{};
+    bool has_sources = false;
+    std::vector<double> track_t, track_x, track_y;
+    double* d_wind = nullptr;      // 4 arrays of (Nx,Ny): U10 theta ustar factor
+    bool wind_field_set = false;
+    // diagnostics scratch
+    double* d_diag = nullptr;      // 5 (Nx,Ny) fields + block partials
+    unsigned int* d_err = nullptr;
+    unsigned int* h_err = nullptr;  // pinned
+    double time = 0.0;
+    int64_t iteration = 0;
+    int64_t bytes = 0;
+};
+
+// ---- launchers (rpl_setup.cu) ----
+cudaError_t launch_doppler(const Handle& h, int64_t Nz, const double* d_u, const double* d_v,
+                           const double* d_zf, const double* d_qdepth, double qdepth_const,
+                           double small_mu, cudaStream_t s);
+cudaError_t launch_gradients(const Handle& h, cudaStream_t s);
+cudaError_t launch_cg_field(const Handle& h, cudaStream_t s);
+cudaError_t launch_wind(const Handle& h, double t, cudaStream_t s);
+cudaError_t launch_stress_factor(const Handle& h, const void* Nin, cudaStream_t s);
+cudaError_t launch_convert(const void* src, int src_dtype, void* dst, int dst_dtype, int64_t n,
+                           cudaStream_t s);
+cudaError_t launch_diagnostics(const Handle& h, const void* Nin, cudaStream_t s);
+cudaError_t launch_scan_nonfinite(const Handle& h, const void* buf, cudaStream_t s);
+
+// ---- stage kernels (rpl_stage.cu) ----
+StageParams make_params(const Handle& h, double dt, int stage);
+cudaError_t launch_stage(const Handle& h, const StageParams& p, const void* Nin, const void* N0,
+                         void* Nout, cudaStream_t s);
+cudaError_t launch_tendency(const Handle& h, const StageParams& p, const void* Nin, double* G,
+                            cudaStream_t s);
+
+}  // namespace rpl

@@ -1,0 +1,416 @@
+// rpl_setup.cu -- set-up and per-step auxiliary kernels: Q-transform Doppler velocity and its
+// kappa derivative, periodic current gradients, finite-depth group speed field, wind fields and
+// the wave-supported stress cap, diagnostics reductions, dtype conversion.
+#include <cuda_runtime.h>
+#include <float.h>
+
+#include <algorithm>
+
+#include "rpl_device.cuh"
+#include "rpl_internal.h"
+
+namespace rpl {
+
+namespace {
+
+// ---------------------------------------------------------------- Q kernel (FP64)
+// CDF of the vertical kernel Q (q_kernel.jl:77-85): F(z) = (e^{2mu(s-1)} - e^{-2mu(s+1)}) /
+// (1 - e^{-4mu}), s = clamp((z+d)/d, 0, 1), mu = kappa*d; F = s when |mu| < small_mu.
+// exact_form = 1 evaluates the exponents as the reference does (2mu*s - 2mu); exact_form = 0
+// evaluates them as 2*kappa*z_c and -2*kappa*(z_c + 2d) with z_c = clamp(z, -d, 0), which avoids
+// the cancellation of 2mu*s - 2mu when kappa*d is large.
+__device__ __forceinline__ double q_cdf(double kappa, double z, double d, double small_mu, int exact_form) {
+    const double mu = kappa * d;
+    const double sgn = mu < 0.0 ? -1.0 : 1.0;
+    const double m = fabs(mu) < small_mu ? sgn * small_mu : mu;
+    double s = (z + d) / d;
+    s = s < 0.0 ? 0.0 : (s > 1.0 ? 1.0 : s);
+    double e1, e2;
+    if (exact_form) {
+        const double a = 2.0 * m * s, b = 2.0 * m;
+        e1 = a - b;
+        e2 = -a - b;
+    } else {
+        const double kq = m / d;  // kappa, or the safe-mu kappa
+        double zc = z < -d ? -d : (z > 0.0 ? 0.0 : z);
+        e1 = 2.0 * kq * zc;
+        e2 = -2.0 * kq * (zc + 2.0 * d);
+    }
+    const double fd = (exp(e1) - exp(e2)) / (1.0 - exp(-4.0 * m));
+    return fabs(mu) < small_mu ? s : fd;
+}
+
+// d F / d kappa (q_kernel.jl:94-109).
+__device__ __forceinline__ double q_cdf_dk(double kappa, double z, double d, double small_mu) {
+    const double mu = kappa * d;
+    const double sgn = mu < 0.0 ? -1.0 : 1.0;
+    const double m = fabs(mu) < small_mu ? sgn * small_mu : mu;
+    double s = (z + d) / d;
+    s = s < 0.0 ? 0.0 : (s > 1.0 ? 1.0 : s);
+    const double small_val = d * (4.0 * mu * s * (s * s - 1.0) / 3.0);
+    const double a = exp(-2.0 * m * (1.0 - s));
+    const double b = exp(-2.0 * m * (1.0 + s));
+    const double e = exp(-4.0 * m);
+    const double num = a - b, den = 1.0 - e;
+    const double dnum = -2.0 * (1.0 - s) * a + 2.0 * (1.0 + s) * b;
+    const double dden = 4.0 * e;
+    const double fd = d * (dnum * den - num * dden) / (den * den);
+    return fabs(mu) < small_mu ? small_val : fd;
+}
+
+// U[i,j,m] = sum_k uL[i,j,k] * (F(z_{k+1}) - F(z_k)) (doppler_velocity.jl:45-62) and the same sum with
+// dF/dkappa (:64-82). One warp per (i,j) column; lanes stride the vertical cells, the partial
+// sums meet in a warp-shuffle reduction.
+__global__ void doppler_kernel(int64_t Nx, int64_t Ny, int64_t Nz, int64_t Nk,
+                               const double* __restrict__ u, const double* __restrict__ v,
+                               const double* __restrict__ zf, const double* __restrict__ qdepth,
+                               double qdepth_const, const double* __restrict__ kappa, double small_mu,
+                               int exact_form, double* __restrict__ Ux, double* __restrict__ Uy,
+                               double* __restrict__ dUx, double* __restrict__ dUy) {
+    const int lane = threadIdx.x & 31;
+    const int64_t col = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (col >= Nx * Ny) return;
+    const double d = qdepth ? qdepth[col] : qdepth_const;
+    const int64_t P = Nx * Ny;
+    for (int64_t m = 0; m < Nk; ++m) {
+        const double kap = kappa[m];
+        double ax = 0.0, ay = 0.0, bx = 0.0, by = 0.0;
+        for (int64_t k = lane; k < Nz; k += 32) {
+            const double lo = fmin(zf[k], zf[k + 1]), hi = fmax(zf[k], zf[k + 1]);
+            const double w = q_cdf(kap, hi, d, small_mu, exact_form) - q_cdf(kap, lo, d, small_mu, exact_form);
+            const double wd = q_cdf_dk(kap, hi, d, small_mu) - q_cdf_dk(kap, lo, d, small_mu);
+            const double uu = u[col + P * k], vv = v[col + P * k];
+            ax += uu * w;
+            ay += vv * w;
+            bx += uu * wd;
+            by += vv * wd;
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            ax += __shfl_down_sync(0xffffffffu, ax, off);
+            ay += __shfl_down_sync(0xffffffffu, ay, off);
+            bx += __shfl_down_sync(0xffffffffu, bx, off);
+            by += __shfl_down_sync(0xffffffffu, by, off);
+        }
+        if (lane == 0) {
+            Ux[col + P * m] = ax;
+            Uy[col + P * m] = ay;
+            dUx[col + P * m] = bx;
+            dUy[col + P * m] = by;
+        }
+    }
+}
+
+// Periodic centred differences of Ux, Uy (wave_current_refraction.jl:7-19).
+__global__ void gradients_kernel(int64_t Nx, int64_t Ny, int64_t Nk, const double* __restrict__ Ux,
+                                 const double* __restrict__ Uy, double dx_inv, double dy_inv,
+                                 double* __restrict__ Uxx, double* __restrict__ Uxy,
+                                 double* __restrict__ Uyx, double* __restrict__ Uyy) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= Nx * Ny * Nk) return;
+    const int64_t i = t % Nx, j = (t / Nx) % Ny, k = t / (Nx * Ny);
+    const int64_t ip = i == Nx - 1 ? 0 : i + 1, im = i == 0 ? Nx - 1 : i - 1;
+    const int64_t jp = j == Ny - 1 ? 0 : j + 1, jm = j == 0 ? Ny - 1 : j - 1;
+    const int64_t o = Nx * Ny * k;
+    Uxx[t] = (Ux[ip + Nx * j + o] - Ux[im + Nx * j + o]) * (dx_inv / 2.0);
+    Uxy[t] = (Ux[i + Nx * jp + o] - Ux[i + Nx * jm + o]) * (dy_inv / 2.0);
+    Uyx[t] = (Uy[ip + Nx * j + o] - Uy[im + Nx * j + o]) * (dx_inv / 2.0);
+    Uyy[t] = (Uy[i + Nx * jp + o] - Uy[i + Nx * jm + o]) * (dy_inv / 2.0);
+}
+
+// Cell-centre finite-depth group speed per (i,j,m) (transport.jl:72-83 without the direction):
+// cg = (1 + 2mu/sinh(2mu))/2 * sqrt(g tanh(mu)/k), mu = k d.
+__global__ void cg_field_kernel(int64_t Nx, int64_t Ny, int64_t Nk, const double* __restrict__ depth,
+                                const double* __restrict__ kappa, double g, double* __restrict__ cg) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= Nx * Ny * Nk) return;
+    const int64_t c = t % (Nx * Ny), m = t / (Nx * Ny);
+    const double k = kappa[m], h = depth[c];
+    const double mu = k * h;
+    const double cp = sqrt(g * tanh(mu) / k);
+    const double gf = (1.0 + 2.0 * mu / sinh(2.0 * mu)) / 2.0;
+    cg[t] = gf * cp;
+}
+
+struct WindArgs {
+    int kind, rotation, drag_form;
+    double speed, direction;
+    double vmax, rmax, radius, shape, inflow, bx, by, cx, cy;  // cx, cy: storm centre at t
+};
+
+__device__ __forceinline__ double friction_velocity(double U, int form) {
+    double cd;
+    if (form == 0) cd = (0.8 + 0.065 * U) * 1e-3;  // drag.jl:77-78
+    else {
+        cd = (8.058 + 0.967 * U - 0.016 * (U * U)) * 1e-4;  // drag.jl:80-83
+        cd = cd > 4e-4 ? cd : 4e-4;
+    }
+    return U * sqrt(cd > 0.0 ? cd : 0.0);
+}
+
+// Per-(i,j) wind speed, direction and friction velocity at one time (winds.jl:255-315,
+// pressure_correlation.jl:54-63, drag.jl:85-86).
+__global__ void wind_kernel(int64_t Nx, int64_t Ny, const double* __restrict__ xn, const double* __restrict__ yn,
+                            WindArgs w, double* __restrict__ U10, double* __restrict__ theta,
+                            double* __restrict__ ustar) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= Nx * Ny) return;
+    double U = 0.0, th = 0.0;
+    if (w.kind == RPL_WIND_UNIFORM) {
+        U = w.speed;
+        th = w.direction;
+    } else if (w.kind == RPL_WIND_HOLLAND) {
+        const double dx = xn[c % Nx] - w.cx, dy = yn[c / Nx] - w.cy;
+        const double r = hypot(dx, dy);
+        double vx = w.bx, vy = w.by;
+        if (r != 0.0) {
+            const double scaled = w.rmax / r;
+            const double shape = pow(scaled, w.shape);
+            const double e = shape * exp(1.0 - shape);
+            double speed = w.vmax * sqrt(e > 0.0 ? e : 0.0);
+            if (r > w.radius) {
+                const double dd = w.radius - w.rmax;
+                const double ulp = nextafter(w.radius, INFINITY) - w.radius;
+                speed *= exp(-(r - w.radius) / (dd > ulp ? dd : ulp));
+            }
+            const double s = (double)w.rotation;
+            const double tx = -s * dy / r, ty = s * dx / r, rx = dx / r, ry = dy / r;
+            const double ci = cos(w.inflow), si = sin(w.inflow);
+            vx = speed * (ci * tx - si * rx) + w.bx;
+            vy = speed * (ci * ty - si * ry) + w.by;
+        }
+        U = hypot(vx, vy);
+        th = atan2(vy, vx);
+    } else if (w.kind == RPL_WIND_FIELD) {
+        U = U10[c];
+        th = theta[c];
+    }
+    U10[c] = U;
+    theta[c] = th;
+    ustar[c] = friction_velocity(U, w.drag_form);
+}
+
+// Wave-supported stress cap per (i,j) (precomputed_sources.jl:282-326): tau_w along the wind from
+// the current spectrum; factor = min(1, 0.4 tau_max / tau_w). Loop n outer, m inner as the reference.
+template <typename T>
+__global__ void stress_kernel(const T* __restrict__ N, StageParams p, double rho_w_g, double rho_air,
+                              double* __restrict__ factor) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t P = p.Nx * p.Ny;
+    if (c >= P) return;
+    const double U = p.wind_U10[c], u_star = p.wind_ustar[c];
+    double f = 1.0;
+    if (U > 0.0 && u_star > 0.0) {
+        const double tu = p.wind_theta[c];
+        const double tau_max = rho_air * (u_star * u_star);
+        double twx = 0.0, twy = 0.0;
+        for (int n = 0; n < p.Np; ++n) {
+            const double cth = p.cosp[n], sth = p.sinp[n];
+            for (int m = 0; m < p.Nk; ++m) {
+                const double a = (double)N[c + P * (m + p.Nk * (int64_t)n)];
+                const double k = p.kappa[m];
+                if (a > 0.0 && k > 0.0) {
+                    const double theta = p.phi[n];
+                    const double rate = jp_rate(k, theta, tu, u_star, p);
+                    if (rate > 0.0) {
+                        const double sigma = sqrt(p.wind_g * k), C = sigma / k;
+                        const double mflux = rate * a / C * p.weights[m + p.Nk * n] * rho_w_g;
+                        twx += mflux * cth;
+                        twy += mflux * sth;
+                    }
+                }
+            }
+        }
+        const double par = twx * cos(tu) + twy * sin(tu);
+        const double eff = par > 0.0 ? par : 0.0;
+        f = (eff > 0.4 * tau_max && tau_max > 0.0) ? 0.4 * tau_max / eff : 1.0;
+    }
+    factor[c] = f;
+}
+
+template <typename S, typename D>
+__global__ void convert_kernel(const S* __restrict__ src, D* __restrict__ dst, int64_t n) {
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
+        dst[t] = (D)src[t];
+}
+
+// Neumaier compensated accumulation.
+__device__ __forceinline__ void kadd(double& s, double& c, double v) {
+    const double t = s + v;
+    if (fabs(s) >= fabs(v)) c += (s - t) + v;
+    else c += (v - t) + s;
+    s = t;
+}
+
+// Per-(i,j) spectral sums (diagnostic_operations.jl:56-165): m0 = sum N w, Hs = 4 sqrt(m0),
+// kappa_rms = sqrt(sum N trace / m0) (0 when m0 = 0), mean direction = atan(sum N mu_y, sum N mu_x).
+template <typename T>
+__global__ void diag_kernel(const T* __restrict__ N, int64_t Nx, int64_t Ny, int64_t Nk, int64_t Np,
+                            const double* __restrict__ tabs, double* __restrict__ out) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t P = Nx * Ny;
+    if (c >= P) return;
+    const int64_t nb = Nk * Np;
+    const double* w = tabs;
+    const double* mux = tabs + nb;
+    const double* muy = tabs + 2 * nb;
+    const double* tr = tabs + 3 * nb;
+    double s0 = 0, c0 = 0, sx = 0, cx = 0, sy = 0, cy = 0, st = 0, ct = 0;
+    for (int64_t b = 0; b < nb; ++b) {
+        const double a = (double)N[c + P * b];
+        kadd(s0, c0, a * w[b]);
+        kadd(sx, cx, a * mux[b]);
+        kadd(sy, cy, a * muy[b]);
+        kadd(st, ct, a * tr[b]);
+    }
+    const double m0 = s0 + c0, mx = sx + cx, my = sy + cy, mt = st + ct;
+    out[c] = m0;
+    out[P + c] = 4.0 * sqrt(m0);
+    out[2 * P + c] = sqrt(m0 == 0.0 ? 0.0 : mt / m0);
+    out[3 * P + c] = atan2(my, mx);
+}
+
+// Total action = sum_ij m0 dx dy with a compensated, deterministic two-level reduction.
+__global__ void total_kernel(const double* __restrict__ m0, int64_t P, double area, double* __restrict__ total) {
+    __shared__ double ss[1024], cc[1024];
+    double s = 0.0, c = 0.0;
+    for (int64_t t = threadIdx.x; t < P; t += blockDim.x) kadd(s, c, m0[t] * area);
+    ss[threadIdx.x] = s;
+    cc[threadIdx.x] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double S = 0.0, C = 0.0;
+        for (unsigned k = 0; k < blockDim.x; ++k) {
+            kadd(S, C, ss[k]);
+            C += cc[k];
+        }
+        *total = S + C;
+    }
+}
+
+template <typename T>
+__global__ void nonfinite_kernel(const T* __restrict__ x, int64_t n, unsigned int* err) {
+    bool bad = false;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
+        bad |= !isfinite(x[t]);
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(err, 2u);
+}
+
+inline unsigned blocks_for(int64_t n, int threads) { return (unsigned)((n + threads - 1) / threads); }
+
+}  // namespace
+
+cudaError_t launch_doppler(const Handle& h, int64_t Nz, const double* d_u, const double* d_v,
+                           const double* d_zf, const double* d_qdepth, double qdepth_const,
+                           double small_mu, cudaStream_t s) {
+    const rpl_desc& d = h.desc;
+    const int64_t c3 = d.Nx * d.Ny * d.Nk;
+    const int64_t cols = d.Nx * d.Ny;
+    const int exact_form = h.precision == RPL_FP64 ? 1 : 0;
+    doppler_kernel<<<blocks_for(cols * 32, 256), 256, 0, s>>>(
+        d.Nx, d.Ny, Nz, d.Nk, d_u, d_v, d_zf, d_qdepth, qdepth_const, h.d_kappa, small_mu, exact_form,
+        h.d_coupling, h.d_coupling + c3, h.d_coupling + 2 * c3, h.d_coupling + 3 * c3);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gradients(const Handle& h, cudaStream_t s) {
+    const rpl_desc& d = h.desc;
+    const int64_t c3 = d.Nx * d.Ny * d.Nk;
+    gradients_kernel<<<blocks_for(c3, 256), 256, 0, s>>>(
+        d.Nx, d.Ny, d.Nk, h.d_coupling, h.d_coupling + c3, 1.0 / d.dx, 1.0 / d.dy, h.d_coupling + 4 * c3,
+        h.d_coupling + 5 * c3, h.d_coupling + 6 * c3, h.d_coupling + 7 * c3);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cg_field(const Handle& h, cudaStream_t s) {
+    const rpl_desc& d = h.desc;
+    const int64_t c3 = d.Nx * d.Ny * d.Nk;
+    cg_field_kernel<<<blocks_for(c3, 256), 256, 0, s>>>(d.Nx, d.Ny, d.Nk, h.d_depth, h.d_kappa, d.gravity,
+                                                         h.d_cgmag);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_wind(const Handle& h, double t, cudaStream_t s) {
+    const rpl_desc& d = h.desc;
+    const int64_t P = d.Nx * d.Ny;
+    WindArgs w{};
+    w.kind = h.src.wind_kind;
+    w.rotation = h.src.rotation;
+    w.drag_form = h.src.drag_form;
+    w.speed = h.src.wind_speed;
+    w.direction = h.src.wind_direction;
+    w.vmax = h.src.vmax; w.rmax = h.src.rmax; w.radius = h.src.radius; w.shape = h.src.shape_parameter;
+    w.inflow = h.src.inflow_angle; w.bx = h.src.background_x; w.by = h.src.background_y;
+    // Storm centre on the LinearStormTrack at t (winds.jl:139-152), host side.
+    const int64_t n = (int64_t)h.track_t.size();
+    if (n == 0) {
+        w.cx = h.track_x.empty() ? 0.0 : h.track_x[0];
+        w.cy = h.track_y.empty() ? 0.0 : h.track_y[0];
+    } else if (t <= h.track_t[0]) {
+        w.cx = h.track_x[0]; w.cy = h.track_y[0];
+    } else if (t >= h.track_t[n - 1]) {
+        w.cx = h.track_x[n - 1]; w.cy = h.track_y[n - 1];
+    } else {
+        int64_t up = 0;
+        while (h.track_t[up] < t) ++up;
+        const int64_t lo = up - 1;
+        const double wt = (t - h.track_t[lo]) / (h.track_t[up] - h.track_t[lo]);
+        w.cx = (1.0 - wt) * h.track_x[lo] + wt * h.track_x[up];
+        w.cy = (1.0 - wt) * h.track_y[lo] + wt * h.track_y[up];
+    }
+    // xnodes / ynodes live after the wind arrays in the same allocation
+    const double* xn = h.d_wind + 4 * P;
+    const double* yn = xn + d.Nx;
+    wind_kernel<<<blocks_for(P, 256), 256, 0, s>>>(d.Nx, d.Ny, xn, yn, w, h.d_wind, h.d_wind + P,
+                                                    h.d_wind + 2 * P);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_stress_factor(const Handle& h, const void* Nin, cudaStream_t s) {
+    const rpl_desc& d = h.desc;
+    const int64_t P = d.Nx * d.Ny;
+    StageParams p = make_params(h, 1.0, 1);
+    const double rho_w_g = h.src.rho_water * h.src.wind_gravity;
+    if (h.precision == RPL_FP64)
+        stress_kernel<double><<<blocks_for(P, 128), 128, 0, s>>>((const double*)Nin, p, rho_w_g, h.src.rho_air,
+                                                                 h.d_wind + 3 * P);
+    else
+        stress_kernel<float><<<blocks_for(P, 128), 128, 0, s>>>((const float*)Nin, p, rho_w_g, h.src.rho_air,
+                                                                h.d_wind + 3 * P);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_convert(const void* src, int src_dtype, void* dst, int dst_dtype, int64_t n, cudaStream_t s) {
+    const unsigned blocks = (unsigned)std::min<int64_t>(blocks_for(n, 256), 148 * 32);
+    if (src_dtype == RPL_F64 && dst_dtype == RPL_F32)
+        convert_kernel<double, float><<<blocks, 256, 0, s>>>((const double*)src, (float*)dst, n);
+    else if (src_dtype == RPL_F32 && dst_dtype == RPL_F64)
+        convert_kernel<float, double><<<blocks, 256, 0, s>>>((const float*)src, (double*)dst, n);
+    else
+        return cudaMemcpyAsync(dst, src, (size_t)n * (src_dtype == RPL_F64 ? 8 : 4), cudaMemcpyDeviceToDevice, s);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_diagnostics(const Handle& h, const void* Nin, cudaStream_t s) {
+    const rpl_desc& d = h.desc;
+    const int64_t P = d.Nx * d.Ny;
+    if (h.precision == RPL_FP64)
+        diag_kernel<double><<<blocks_for(P, 128), 128, 0, s>>>((const double*)Nin, d.Nx, d.Ny, d.Nk, d.Np,
+                                                               h.d_weights, h.d_diag);
+    else
+        diag_kernel<float><<<blocks_for(P, 128), 128, 0, s>>>((const float*)Nin, d.Nx, d.Ny, d.Nk, d.Np,
+                                                              h.d_weights, h.d_diag);
+    total_kernel<<<1, 1024, 0, s>>>(h.d_diag, P, d.dx * d.dy, h.d_diag + 4 * P);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_scan_nonfinite(const Handle& h, const void* buf, cudaStream_t s) {
+    const unsigned blocks = (unsigned)std::min<int64_t>(blocks_for(h.units, 256), 148 * 32);
+    if (h.precision == RPL_FP64)
+        nonfinite_kernel<double><<<blocks, 256, 0, s>>>((const double*)buf, h.units, h.d_err);
+    else
+        nonfinite_kernel<float><<<blocks, 256, 0, s>>>((const float*)buf, h.units, h.d_err);
+    return cudaGetLastError();
+}
+
+}  // namespace rpl

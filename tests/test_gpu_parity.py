@@ -1,0 +1,244 @@
+"""Parity of the CUDA path (librpl.so through the C-ABI) with the CPU FP64 oracle.
+
+Tolerances: the FP64 path must match the oracle to rel-L2 <= 1e-12 on the action after
+the run; the FP32 precision form to rel-L2 <= 1e-5 (both stated by the benchmark
+contract). Tendencies and set-up fields are compared at 1e-13 of their maximum.
+"""
+import ctypes
+import math
+import os
+import sys
+
+import numpy as np
+import pytest
+
+import ripple_b200 as rp
+from ripple_b200 import _lib, workloads
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+sys.path.insert(0, GOLDEN)
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+
+FP64_TOL = 1e-12
+FP32_TOL = 1e-5
+
+
+def rel_l2(a, b):
+    a, b = np.ravel(a), np.ravel(b)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def run_both(oracle_mod, w, nsteps, precision="fp64", **kw):
+    m = w.model(precision, **kw)
+    rp.time_step(m, w.dt, nsteps)
+    Ng = m.action.interior()
+    No, t = oracle_mod.Oracle(w).step(w.N0, w.dt, nsteps)
+    assert m.clock.time == pytest.approx(t, rel=1e-15)
+    assert m.clock.iteration == nsteps
+    return m, Ng, No
+
+
+def test_kat_tendency_matches_golden(oracle_mod):
+    from make_golden import kat_workload
+    ref = np.load(os.path.join(GOLDEN, "kat_tendency_8x7x4x6.npz"))
+    k = kat_workload()
+    m = k.model("fp64")
+    G = rp.interior(rp.compute_tendencies(m))
+    assert np.max(np.abs(G - ref["G"])) <= 1e-13 * np.max(np.abs(ref["G"]))
+
+
+def test_coupling_fields_match_oracle(oracle_mod):
+    from make_golden import kat_workload
+    for w in (kat_workload(), workloads.seamount_eddies(N=24, Nz=32, Nk=8, Np=12, nsteps=1)):
+        m = w.model("fp64")
+        got = m.coupling_fields()
+        o = oracle_mod.Oracle(w)
+        ref = o.coupling(got["Ux"].shape)
+        for name in ("Ux", "Uy", "dUxdkappa", "dUydkappa", "Ux_x", "Ux_y", "Uy_x", "Uy_y"):
+            scale = max(np.max(np.abs(ref[name])), 1e-300)
+            assert np.max(np.abs(got[name] - ref[name])) <= 1e-13 * scale, name
+
+
+def test_vortex_refraction_reduced_fp64(oracle_mod):
+    w = workloads.vortex_refraction(N=16, nsteps=40)
+    m, Ng, No = run_both(oracle_mod, w, 40)
+    assert rel_l2(Ng, No) <= FP64_TOL
+    assert Ng.min() >= 0
+
+
+@pytest.mark.slow
+def test_vortex_refraction_full_run_matches_golden(oracle_mod):
+    """The full vortex-refraction configuration (400 steps) against the oracle's golden output."""
+    ref = np.load(os.path.join(GOLDEN, "c1_vortex_refraction.npz"))
+    w = workloads.vortex_refraction()
+    m = w.model("fp64")
+    sim = rp.Simulation(m, Δt=w.dt, stop_iteration=w.nsteps)
+    rp.run_(sim)
+    N = m.action.interior().ravel(order="F")
+    assert rel_l2(N[::97], ref["sample"]) <= FP64_TOL
+    assert abs(N.sum() - float(ref["sum"])) <= FP64_TOL * abs(float(ref["sum"]))
+    d = rp.diagnostics(m.action)
+    assert rel_l2(d["m0"], ref["m0"]) <= FP64_TOL
+    assert rel_l2(d["kappa_rms"], ref["kappa_rms"]) <= FP64_TOL
+    assert np.max(np.abs(d["mean_direction"] - ref["mean_direction"])) <= 1e-10
+    assert d["total_action"] == pytest.approx(float(ref["total_action"]), rel=FP64_TOL)
+    # and against a fresh oracle run of the same configuration
+    No, _ = oracle_mod.Oracle(w).step(w.N0, w.dt, w.nsteps)
+    assert rel_l2(N, No.ravel(order="F")) <= FP64_TOL
+
+
+def test_vortex_refraction_fp32(oracle_mod):
+    w = workloads.vortex_refraction(N=32, nsteps=40)
+    m, Ng, No = run_both(oracle_mod, w, 40, precision="fp32")
+    assert rel_l2(Ng, No) <= FP32_TOL
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", FP64_TOL), ("fp32", FP32_TOL)])
+def test_seamount_eddies_reduced(oracle_mod, precision, tol):
+    w = workloads.seamount_eddies(N=40, Nz=32, Nk=32, Np=36, nsteps=4)
+    m, Ng, No = run_both(oracle_mod, w, 4, precision=precision)
+    assert rel_l2(Ng, No) <= tol
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", FP64_TOL), ("fp32", FP32_TOL)])
+def test_hurricane_sources_reduced(oracle_mod, precision, tol):
+    w = workloads.hurricane_swell(N=40, Nk=32, Np=36, nsteps=4, dx=25000.0)
+    m, Ng, No = run_both(oracle_mod, w, 4, precision=precision)
+    assert rel_l2(Ng, No) <= tol
+    assert np.max(np.abs(Ng - No)) > 0 or precision == "fp64"
+
+
+def test_stress_factor_and_wind_match_oracle(oracle_mod):
+    w = workloads.hurricane_swell(N=24, Nk=16, Np=24, nsteps=2, dx=40000.0)
+    rng = np.random.default_rng(5)
+    w.N0 = np.asfortranarray(rng.uniform(0.0, 2.0, w.N0.shape))
+    m = w.model("fp64")
+    G = rp.interior(rp.compute_tendencies(m))
+    Go = oracle_mod.Oracle(w).tendency(w.N0)
+    assert np.max(np.abs(G - Go)) <= 1e-12 * np.max(np.abs(Go))
+
+
+@pytest.mark.parametrize("axis", ["x", "y"])
+def test_weno_sinusoid_on_gpu(axis):
+    from test_oracle_golden import sinusoid_workload
+    w = sinusoid_workload(axis)
+    m = w.model("fp64")
+    G = rp.interior(rp.compute_tendencies(m))
+    L = 64.0
+    import oracle as O
+    o = O.Oracle(w, explicit_spectral_faces=True)
+    if axis == "x":
+        o_u = o._cg[0][0]
+        exp = -o_u * 0.1 * 2 * math.pi / L * np.cos(2 * math.pi * w.grid.xnodes() / L)[:, None]
+    else:
+        o_u = o._cg[1][0]
+        exp = -o_u * 0.1 * 2 * math.pi / L * np.cos(2 * math.pi * w.grid.ynodes() / L)[None, :]
+    assert np.max(np.abs(G[:, :, 0, 0] - exp)) < 1e-7
+    tot0 = rp.total_action(m.action)
+    rp.time_step(m, 0.1)
+    assert abs(rp.total_action(m.action) - tot0) <= 1e-10
+    assert m.action.interior().min() > 0
+
+
+def test_rk3_linear_column_on_gpu():
+    from test_oracle_golden import linear_damping_workload
+    w = linear_damping_workload()
+    m = w.model("fp64")
+    rp.time_step(m, 0.1, nsteps=3)
+    N = m.action.interior()
+    for mm, k in enumerate((0.5, 1.0)):
+        z = 0.4 * math.sqrt(9.81 * k) * 0.1
+        amp = 1 - z + z * z / 2 - z ** 3 / 6
+        assert N[0, 0, mm, 0] == pytest.approx(50.0 * amp ** 3, rel=1e-14)
+
+
+def test_wind_input_signs_on_gpu():
+    from test_oracle_golden import wind_column_workload
+    w = wind_column_workload(15.0)
+    G = rp.interior(rp.compute_tendencies(w.model("fp64")))
+    assert G.max() > 0 and G.min() >= 0
+    calm = wind_column_workload(0.0)
+    assert np.all(rp.interior(rp.compute_tendencies(calm.model("fp64"))) == 0)
+
+
+def test_diagnostics_match_oracle(oracle_mod):
+    w = workloads.seamount_eddies(N=24, Nz=8, Nk=32, Np=36, nsteps=1)
+    m = w.model("fp64")
+    d = rp.diagnostics(m.action)
+    do = oracle_mod.Oracle(w).diagnostics(w.N0)
+    for k in ("m0", "Hs", "kappa_rms"):
+        assert rel_l2(d[k], do[k]) <= 1e-14, k
+    assert np.max(np.abs(d["mean_direction"] - do["mean_direction"])) <= 1e-13
+    assert d["total_action"] == pytest.approx(do["total_action"], rel=1e-14)
+
+
+@pytest.mark.parametrize("shape", [(3, 5, 1, 3), (37, 29, 5, 7), (33, 3, 2, 4)])
+def test_edge_sizes_refraction(oracle_mod, shape):
+    Nx, Ny, Nk, Np = shape
+    rng = np.random.default_rng(sum(shape))
+    g = rp.RectilinearGrid(size=(Nx, Ny, 4), x=(0.0, Nx * 2.0), y=(0.0, Ny * 2.0), z=(-3.0, 0.0))
+    sg = rp.PolarWaveVectorGrid(κ=np.linspace(0.3, 0.9, Nk), φ=np.arange(Np) * 2 * math.pi / Np)
+    u = np.asfortranarray(rng.uniform(-0.3, 0.3, (Nx, Ny, 4)))
+    v = np.asfortranarray(rng.uniform(-0.3, 0.3, (Nx, Ny, 4)))
+    N0 = np.asfortranarray(rng.uniform(0.0, 1.0, shape))
+    w = workloads.Workload("edge", g, sg, 2.0, N0, 0.05, 3, velocities={"u": u, "v": v})
+    m, Ng, No = run_both(oracle_mod, w, 3)
+    assert rel_l2(Ng, No) <= FP64_TOL
+
+
+def test_set_get_roundtrip_and_clock():
+    w = workloads.seamount_eddies(N=16, Nz=4, Nk=4, Np=6, nsteps=1)
+    for precision in ("fp64", "fp32"):
+        m = w.model(precision)
+        got = m.action.interior()
+        if precision == "fp64":
+            assert np.array_equal(got, w.N0)
+        else:
+            assert np.array_equal(got, w.N0.astype(np.float32).astype(np.float64))
+        m.clock.time = 12.5
+        rp.time_step(m, 0.5)
+        assert m.clock.time == 13.0 and m.clock.iteration == 1
+
+
+def test_error_paths():
+    w = workloads.seamount_eddies(N=16, Nz=4, Nk=4, Np=6, nsteps=1)
+    m = w.model("fp64")
+    with pytest.raises(rp.ArgumentError):
+        rp.time_step(m, 0.0)
+    with pytest.raises(rp.ArgumentError):
+        rp.time_step(m, -1.0)
+    bad = w.N0.copy(order="F")
+    bad[3, 2, 1, 0] = np.nan
+    with pytest.raises(rp.RplError) as e:
+        m.action.set(bad)
+    assert e.value.code == _lib.RPL_ERR_NONFINITE
+    # a huge step drives the action to overflow; the kernels' error word reports it
+    m.action.set(w.N0 * 1e300)
+    with pytest.raises(rp.RplError) as e:
+        rp.time_step(m, 1e12)
+    assert e.value.code == _lib.RPL_ERR_DEVICE
+    # the handle stays usable afterwards
+    m.action.set(w.N0)
+    rp.time_step(m, w.dt)
+    assert np.all(np.isfinite(m.action.interior()))
+    # refraction transport without currents is refused
+    lib = _lib.load()
+    d = _lib.RplDesc()
+    keep = dict(x=np.arange(4.0) + 0.5, k=np.array([0.5]), kf=np.array([0.4, 0.6]), p=np.array([0.0, 2.0, 4.0]),
+                pf=np.array([-1.0, 1.0, 3.0, 5.0]))
+    d.abi_version, d.precision, d.transport = _lib.RPL_ABI_VERSION, _lib.RPL_FP64, _lib.RPL_TRANSPORT_REFRACTION
+    d.Nx = d.Ny = 4
+    d.Nk, d.Np = 1, 3
+    d.dx = d.dy = 1.0
+    d.xnodes = d.ynodes = _lib.dptr(keep["x"])
+    d.periodic_x = d.periodic_y = 1
+    d.kappa, d.kappa_faces, d.phi, d.phi_faces = (_lib.dptr(keep[k]) for k in ("k", "kf", "p", "pf"))
+    d.gravity = 9.81
+    h = ctypes.c_void_p()
+    assert lib.rpl_create(ctypes.byref(d), ctypes.byref(h)) == _lib.RPL_OK
+    assert lib.rpl_step(h, 0.1, 1) == _lib.RPL_ERR_STATE
+    assert lib.rpl_stage_async(h, 0.1, 4) == _lib.RPL_ERR_STATE
+    assert lib.rpl_destroy(h) == _lib.RPL_OK
