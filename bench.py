@@ -179,6 +179,10 @@ def run_ours(args, rank, world, local_rank):
             dist.barrier()
         torch.cuda.synchronize()
 
+    try:
+        smi_id = "GPU-" + str(torch.cuda.get_device_properties(local_rank).uuid)
+    except Exception:
+        smi_id = str(local_rank)
     w = workloads.seamount_eddies(N=args.size, Nz=32, Nk=32, Np=36, nsteps=args.steps, n0_dtype=np.float32)
     m = w.model(args.precision, device=local_rank)
     lib, h = m._lib, m.handle
@@ -195,7 +199,7 @@ def run_ours(args, rank, world, local_rank):
     # device-timed region: K steps, events around each stage launch on the launching stream
     ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local_rank) as clk:
+    with ClockSampler(smi_id) as clk:
         barrier()
         with torch.cuda.stream(torch_stream):
             start.record(torch_stream)

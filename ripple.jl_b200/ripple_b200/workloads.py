@@ -94,8 +94,10 @@ def jonswap_spectrum(kappa, phi, kp=0.03, gamma=3.3, s=10, phi0=math.pi / 4):
     return np.outer(E, D)
 
 
-def seamount_eddies(N=1024, Nz=32, Nk=32, Np=36, nsteps=200, seed=2, dx=5000.0, cfl=0.4, n0_dtype=np.float64):
-    L = N * dx
+def seamount_eddies(N=1024, Nz=32, Nk=32, Np=36, nsteps=200, seed=2, L=1024 * 5000.0, cfl=0.4,
+                    n0_dtype=np.float64):
+    """Reduced N keeps the 5120 km domain (coarser cells), so seamounts and eddies keep their extent."""
+    dx = L / N
     grid = RectilinearGrid(size=(N, N, Nz), x=(0.0, L), y=(0.0, L), z=(-4000.0, 0.0),
                            topology=("Periodic", "Periodic", "Bounded"))
     kappa = np.geomspace(0.002, 0.5, Nk)
@@ -146,8 +148,9 @@ def seamount_eddies(N=1024, Nz=32, Nk=32, Np=36, nsteps=200, seed=2, dx=5000.0, 
                            "N0": "JONSWAP kp=0.03 gamma=3.3, cos^20((phi-pi/4)/2), x-y envelope 1+0.3 sin cos"})
 
 
-def hurricane_swell(N=768, Nk=32, Np=36, nsteps=1000, dx=10000.0, cfl=0.4, translation=5.0, Nz=24):
-    L = N * dx
+def hurricane_swell(N=768, Nk=32, Np=36, nsteps=1000, L=768 * 10000.0, cfl=0.4, translation=5.0, Nz=24):
+    """Reduced N keeps the 7680 km domain (coarser cells)."""
+    dx = L / N
     grid = RectilinearGrid(size=(N, N, Nz), x=(0.0, L), y=(0.0, L), z=(-4000.0, 0.0),
                            topology=("Periodic", "Periodic", "Bounded"))
     kappa = np.geomspace(0.003, 0.3, Nk)

@@ -58,7 +58,7 @@ def test_coupling_fields_match_oracle(oracle_mod):
         o = oracle_mod.Oracle(w)
         ref = o.coupling(got["Ux"].shape)
         for name in ("Ux", "Uy", "dUxdkappa", "dUydkappa", "Ux_x", "Ux_y", "Uy_x", "Uy_y"):
-            scale = max(np.max(np.abs(ref[name])), 1e-300)
+            scale = max(np.max(np.abs(ref[name])), np.max(np.abs(ref["Ux"])))
             assert np.max(np.abs(got[name] - ref[name])) <= 1e-13 * scale, name
 
 
@@ -105,14 +105,14 @@ def test_seamount_eddies_reduced(oracle_mod, precision, tol):
 
 @pytest.mark.parametrize("precision,tol", [("fp64", FP64_TOL), ("fp32", FP32_TOL)])
 def test_hurricane_sources_reduced(oracle_mod, precision, tol):
-    w = workloads.hurricane_swell(N=40, Nk=32, Np=36, nsteps=4, dx=25000.0)
+    w = workloads.hurricane_swell(N=48, Nk=32, Np=36, nsteps=4)
     m, Ng, No = run_both(oracle_mod, w, 4, precision=precision)
     assert rel_l2(Ng, No) <= tol
     assert np.max(np.abs(Ng - No)) > 0 or precision == "fp64"
 
 
 def test_stress_factor_and_wind_match_oracle(oracle_mod):
-    w = workloads.hurricane_swell(N=24, Nk=16, Np=24, nsteps=2, dx=40000.0)
+    w = workloads.hurricane_swell(N=24, Nk=16, Np=24, nsteps=2)
     rng = np.random.default_rng(5)
     w.N0 = np.asfortranarray(rng.uniform(0.0, 2.0, w.N0.shape))
     m = w.model("fp64")
