@@ -171,6 +171,28 @@ int rpl_tendency(rpl_handle* h, double* G, int32_t layout);
 int rpl_diagnostics(rpl_handle* h, double* m0, double* hs, double* krms, double* mean_dir,
                     double* total_action);
 
+/* Largest Nx*Ny that rpl_diagnostics_static accepts (2048 x 2048 cells). */
+#define RPL_STATIC_MAX_COLUMNS 4194304
+
+/* No counterpart in the reference. The diagnostics of rpl_diagnostics for a wave action the caller
+ * already holds on the device, for callers that must not allocate device memory when they ask for
+ * them: a host framework whose device memory belongs entirely to its own pool allocator (Julia's
+ * CUDA.jl pool, PyTorch's caching allocator), or work enqueued while such a framework captures a
+ * stream. Needs no handle and allocates nothing: every pointer is device memory on the calling
+ * thread's current device. N: (Nx,Ny,Nk,Np) RPL_LAYOUT_XFAST of dtype; measures: 4*Nk*Np FP64 in
+ * the order spectral weights, first-moment x, first-moment y, second-moment trace (each (Nk,Np),
+ * kappa fastest; polar_wavevector_grid.jl:44-47,73-115); outputs m0, hs, krms, mean_dir ((Nx,Ny))
+ * and total (1 value) may each be NULL. Kernels go on `stream` (a cudaStream_t, NULL = default).
+ * The only scratch, the per-block partial sums of the total action, is a fixed 256 KiB array inside
+ * the library that every GPU loading librpl.so keeps until the process exits, so Nx*Ny is limited to
+ * RPL_STATIC_MAX_COLUMNS (larger grids return RPL_ERR_ARGUMENT). Every call reuses that array, so
+ * calls that may overlap on the GPU (different streams, different host threads) race and must be
+ * ordered by the caller. The first call on each device looks up the array's device address and may
+ * load the library's kernels onto that device; make that first call before any stream capture. */
+int rpl_diagnostics_static(const void* N, int32_t dtype, int64_t Nx, int64_t Ny, int64_t Nk, int64_t Np,
+                           const double* measures, double dx, double dy, double* m0, double* hs,
+                           double* krms, double* mean_dir, double* total, void* stream);
+
 /* Device bytes held by the handle. */
 int rpl_device_bytes(rpl_handle* h, int64_t* bytes);
 /* Thread-local message of the last failing call on this thread ("" if none). */

@@ -130,6 +130,8 @@ int check_step_args(Handle* h, double dt) {
 
 }  // namespace
 
+void rpl::set_last_error(const std::string& msg) { g_last_error = msg; }
+
 extern "C" {
 
 const char* rpl_last_error(void) { return g_last_error.c_str(); }

@@ -86,6 +86,9 @@ struct Handle {
     int64_t bytes = 0;
 };
 
+// Sets the thread-local message rpl_last_error() returns (rpl_api.cu).
+void set_last_error(const std::string& msg);
+
 // ---- launchers (rpl_setup.cu) ----
 cudaError_t launch_doppler(const Handle& h, int64_t Nz, const double* d_u, const double* d_v,
                            const double* d_zf, const double* d_qdepth, double qdepth_const,

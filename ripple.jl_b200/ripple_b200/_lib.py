@@ -88,6 +88,8 @@ _SIGNATURES = {
     "rpl_tendency": (ctypes.c_int, [ctypes.c_void_p, _dp, _i32]),
     "rpl_diagnostics": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp, _dp, _dp, _dp]),
     "rpl_device_bytes": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(_i64)]),
+    "rpl_diagnostics_static": (ctypes.c_int, [ctypes.c_void_p, _i32, _i64, _i64, _i64, _i64, ctypes.c_void_p,
+                                              _d, _d] + [ctypes.c_void_p] * 6),
     "rpl_last_error": (ctypes.c_char_p, []),
     "rpl_abi_version": (ctypes.c_int, []),
 }
