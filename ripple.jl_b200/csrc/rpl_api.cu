@@ -69,7 +69,8 @@ cudaError_t dalloc(Handle* h, T** p, size_t count) {
 
 void free_all(Handle* h) {
     void* ptrs[] = {h->N, h->A, h->B, h->d_kappa, h->d_phi, h->d_cos, h->d_sin, h->d_weights, h->d_cgx,
-                    h->d_cgy, h->d_cgmag, h->d_depth, h->d_coupling, h->d_wind, h->d_diag, h->d_err};
+                    h->d_cgy, h->d_cgmag, h->d_depth, h->d_coupling, h->d_wind, h->d_diag, h->d_err,
+                    h->d_coef, h->d_tab32};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->h_err) cudaFreeHost(h->h_err);
@@ -186,7 +187,7 @@ int rpl_create(const rpl_desc* d, rpl_handle** out) {
     const int64_t units = d->Nx * d->Ny * d->Nk * d->Np;
     const size_t elem = d->precision == RPL_FP64 ? 8 : 4;
     const int64_t c3 = d->Nx * d->Ny * d->Nk, P = d->Nx * d->Ny, nb = d->Nk * d->Np;
-    int64_t need = 3 * units * (int64_t)elem + 8 * c3 * 8 + (d->depth_kind == RPL_DEPTH_FIELD ? (c3 + P) * 8 : 0) +
+    int64_t need = 3 * units * (int64_t)elem + 16 * c3 * 8 + (d->depth_kind == RPL_DEPTH_FIELD ? (c3 + P) * 8 : 0) +
                    (4 * P + d->Nx + d->Ny) * 8 + 6 * P * 8 + 8 * nb * 8;
     if (d->memory_limit_bytes > 0 && need > d->memory_limit_bytes)
         return fail(RPL_ERR_OOM, "model needs " + std::to_string(need) + " device bytes, above the memory limit of " +
@@ -304,6 +305,25 @@ int rpl_create(const rpl_desc* d, rpl_handle** out) {
         TRY(cudaMemcpyAsync(h->d_depth, h->depth_field.data(), P * 8, cudaMemcpyHostToDevice, s));
         TRY(rpl::launch_cg_field(*h, s));
     }
+    TRY(dalloc(h, &h->d_coef, 8 * c3));
+    TRY(rpl::launch_coef(*h, s));
+    {
+        std::vector<float> tab32(4 * d->Np + 2 * nb);
+        for (int64_t n = 0; n < d->Np; ++n) {
+            const float c = (float)cosp[n], sn = (float)sinp[n];
+            tab32[4 * n] = c * c;
+            tab32[4 * n + 1] = c * sn;
+            tab32[4 * n + 2] = sn * sn;
+            tab32[4 * n + 3] = 0.0f;
+        }
+        for (int64_t b = 0; b < nb; ++b) {
+            tab32[4 * d->Np + 2 * b] = (float)cgx[b];
+            tab32[4 * d->Np + 2 * b + 1] = (float)cgy[b];
+        }
+        TRY(dalloc(h, &h->d_tab32, tab32.size()));
+        TRY(cudaMemcpyAsync(h->d_tab32, tab32.data(), tab32.size() * 4, cudaMemcpyHostToDevice, s));
+        TRY(cudaStreamSynchronize(s));
+    }
     TRY(cudaStreamSynchronize(s));
 #undef TRY
     *out = reinterpret_cast<rpl_handle*>(h);
@@ -359,12 +379,19 @@ int rpl_set_currents(rpl_handle* hh, int64_t Nz, const double* z_faces, int32_t 
     if (e == cudaSuccess && dq) e = cudaMemcpyAsync(dq, q_depth_field, P * 8, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = rpl::launch_doppler(*h, Nz, du, dv, dz, dq, q_depth_constant, small_mu, s);
     if (e == cudaSuccess) e = rpl::launch_gradients(*h, s);
+    if (e == cudaSuccess) {
+        h->currents_set = true;  // the coefficient records read the coupling from here on
+        e = rpl::launch_coef(*h, s);
+    }
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     cudaFree(du);
     cudaFree(dv);
     cudaFree(dz);
     if (dq) cudaFree(dq);
-    if (e != cudaSuccess) return cuda_fail(e, "rpl_set_currents");
+    if (e != cudaSuccess) {
+        h->currents_set = false;
+        return cuda_fail(e, "rpl_set_currents");
+    }
     h->currents_set = true;
     return RPL_OK;
 }
@@ -465,16 +492,29 @@ static int set_action_impl(Handle* h, const void* N, int32_t dtype, int32_t layo
     const int64_t n = h->units;
     const size_t src_elem = dtype == RPL_F64 ? 8 : 4;
     const int state_dtype = h->precision == RPL_FP64 ? RPL_F64 : RPL_F32;
-    const cudaMemcpyKind kind = device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-    if (dtype == state_dtype) {
-        RPL_CUDA(cudaMemcpyAsync(h->N, N, n * src_elem, kind, s));
+    const int64_t Nk = h->desc.Nk, Np = h->desc.Np, P = h->cells, slice = P * Nk;
+    if (device) {
+        RPL_CUDA(rpl::launch_to_device_layout(*h, N, dtype, h->N, state_dtype, 0, Np, 0, Nk, s));
     } else {
-        // stage through buffer A (free between steps), converting chunk by chunk
-        const int64_t chunk = (int64_t)(h->units * h->elem / src_elem);
-        for (int64_t off = 0; off < n; off += chunk) {
-            const int64_t cnt = std::min<int64_t>(chunk, n - off);
-            RPL_CUDA(cudaMemcpyAsync(h->A, (const char*)N + off * src_elem, cnt * src_elem, kind, s));
-            RPL_CUDA(rpl::launch_convert(h->A, dtype, (char*)h->N + off * h->elem, state_dtype, cnt, s));
+        // staged through buffer A (free between steps), transposed into the device layout chunk by chunk
+        const int64_t cap = (int64_t)(h->units * h->elem / src_elem);  // source elements that fit in A
+        if (cap >= slice) {
+            const int64_t per = cap / slice;
+            for (int64_t n0 = 0; n0 < Np; n0 += per) {
+                const int64_t nc = std::min<int64_t>(per, Np - n0);
+                RPL_CUDA(cudaMemcpyAsync(h->A, (const char*)N + n0 * slice * src_elem, nc * slice * src_elem,
+                                         cudaMemcpyHostToDevice, s));
+                RPL_CUDA(rpl::launch_to_device_layout(*h, h->A, dtype, h->N, state_dtype, n0, nc, 0, Nk, s));
+            }
+        } else {
+            const int64_t rows = std::max<int64_t>(1, cap / P);
+            for (int64_t n0 = 0; n0 < Np; ++n0)
+                for (int64_t m0 = 0; m0 < Nk; m0 += rows) {
+                    const int64_t mc = std::min<int64_t>(rows, Nk - m0);
+                    RPL_CUDA(cudaMemcpyAsync(h->A, (const char*)N + (n0 * slice + m0 * P) * src_elem,
+                                             mc * P * src_elem, cudaMemcpyHostToDevice, s));
+                    RPL_CUDA(rpl::launch_to_device_layout(*h, h->A, dtype, h->N, state_dtype, n0, 1, m0, mc, s));
+                }
         }
     }
     RPL_CUDA(rpl::launch_scan_nonfinite(*h, h->N, s));
@@ -494,15 +534,29 @@ static int get_action_impl(Handle* h, void* N, int32_t dtype, int32_t layout, bo
     const int64_t n = h->units;
     const size_t dst_elem = dtype == RPL_F64 ? 8 : 4;
     const int state_dtype = h->precision == RPL_FP64 ? RPL_F64 : RPL_F32;
-    const cudaMemcpyKind kind = device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
-    if (dtype == state_dtype) {
-        RPL_CUDA(cudaMemcpyAsync(N, h->N, n * dst_elem, kind, s));
+    (void)n;
+    const int64_t Nk = h->desc.Nk, Np = h->desc.Np, P = h->cells, slice = P * Nk;
+    if (device) {
+        RPL_CUDA(rpl::launch_from_device_layout(*h, h->N, state_dtype, N, dtype, 0, Np, 0, Nk, s));
     } else {
-        const int64_t chunk = (int64_t)(h->units * h->elem / dst_elem);
-        for (int64_t off = 0; off < n; off += chunk) {
-            const int64_t cnt = std::min<int64_t>(chunk, n - off);
-            RPL_CUDA(rpl::launch_convert((const char*)h->N + off * h->elem, state_dtype, h->A, dtype, cnt, s));
-            RPL_CUDA(cudaMemcpyAsync((char*)N + off * dst_elem, h->A, cnt * dst_elem, kind, s));
+        const int64_t cap = (int64_t)(h->units * h->elem / dst_elem);  // destination elements that fit in A
+        if (cap >= slice) {
+            const int64_t per = cap / slice;
+            for (int64_t n0 = 0; n0 < Np; n0 += per) {
+                const int64_t nc = std::min<int64_t>(per, Np - n0);
+                RPL_CUDA(rpl::launch_from_device_layout(*h, h->N, state_dtype, h->A, dtype, n0, nc, 0, Nk, s));
+                RPL_CUDA(cudaMemcpyAsync((char*)N + n0 * slice * dst_elem, h->A, nc * slice * dst_elem,
+                                         cudaMemcpyDeviceToHost, s));
+            }
+        } else {
+            const int64_t rows = std::max<int64_t>(1, cap / P);
+            for (int64_t n0 = 0; n0 < Np; ++n0)
+                for (int64_t m0 = 0; m0 < Nk; m0 += rows) {
+                    const int64_t mc = std::min<int64_t>(rows, Nk - m0);
+                    RPL_CUDA(rpl::launch_from_device_layout(*h, h->N, state_dtype, h->A, dtype, n0, 1, m0, mc, s));
+                    RPL_CUDA(cudaMemcpyAsync((char*)N + (n0 * slice + m0 * P) * dst_elem, h->A, mc * P * dst_elem,
+                                             cudaMemcpyDeviceToHost, s));
+                }
         }
     }
     RPL_CUDA(cudaStreamSynchronize(s));
@@ -610,17 +664,20 @@ int rpl_tendency(rpl_handle* hh, double* G, int32_t layout) {
     if (layout != RPL_LAYOUT_XFAST) return fail(RPL_ERR_ARGUMENT, "unknown layout");
     if ((st = check_step_args(h, 1.0))) return st;
     cudaStream_t s = h->stream;
-    double* dG = nullptr;
+    double *dG = nullptr, *dGx = nullptr;
     RPL_CUDA(cudaMalloc(&dG, h->units * 8));
-    cudaError_t e = cudaSuccess;
-    if (h->has_sources && h->src.wind_kind != RPL_WIND_NONE) {
+    cudaError_t e = cudaMalloc(&dGx, h->units * 8);
+    if (e == cudaSuccess && h->has_sources && h->src.wind_kind != RPL_WIND_NONE) {
         e = rpl::launch_wind(*h, h->time, s);
         if (e == cudaSuccess && h->src.stress_cap) e = rpl::launch_stress_factor(*h, h->N, s);
     }
     if (e == cudaSuccess) e = rpl::launch_tendency(*h, rpl::make_params(*h, 1.0, 1), h->N, dG, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(G, dG, h->units * 8, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess)
+        e = rpl::launch_from_device_layout(*h, dG, RPL_F64, dGx, RPL_F64, 0, h->desc.Np, 0, h->desc.Nk, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(G, dGx, h->units * 8, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     cudaFree(dG);
+    if (dGx) cudaFree(dGx);
     if (e != cudaSuccess) return cuda_fail(e, "rpl_tendency");
     return RPL_OK;
 }

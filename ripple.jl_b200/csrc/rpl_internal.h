@@ -35,6 +35,9 @@ struct StageParams {
     const double* Uxy;
     const double* Uyx;
     const double* Uyy;
+    const double* coef;                     // per (i,j,m) device order: 8 doubles (see rpl_layout.cu)
+    const float4* trig32;                   // Np: (cos^2, cos*sin, sin^2, 0) of each direction, FP32
+    const float2* cg32;                     // (Nk,Np): the cg_x, cg_y table entries rounded to FP32
     // sources
     int has_wind, stress_cap, has_diss;
     const double* wind_U10;                 // (Nx,Ny)
@@ -70,6 +73,8 @@ struct Handle {
     double* d_cgmag = nullptr;
     double* d_depth = nullptr;
     double* d_coupling = nullptr;  // 8 arrays of (Nx,Ny,Nk): Ux Uy dUxdk dUydk Uxx Uxy Uyx Uyy
+    double* d_coef = nullptr;      // (Nx*Ny*Nk) records of 8 doubles in device order
+    float* d_tab32 = nullptr;      // 4*Np trig entries, then 2*Nk*Np group-velocity entries (FP32 copies)
     bool currents_set = false;
     // sources
     rpl_sources src{};
@@ -97,10 +102,15 @@ cudaError_t launch_gradients(const Handle& h, cudaStream_t s);
 cudaError_t launch_cg_field(const Handle& h, cudaStream_t s);
 cudaError_t launch_wind(const Handle& h, double t, cudaStream_t s);
 cudaError_t launch_stress_factor(const Handle& h, const void* Nin, cudaStream_t s);
-cudaError_t launch_convert(const void* src, int src_dtype, void* dst, int dst_dtype, int64_t n,
-                           cudaStream_t s);
 cudaError_t launch_diagnostics(const Handle& h, const void* Nin, cudaStream_t s);
 cudaError_t launch_scan_nonfinite(const Handle& h, const void* buf, cudaStream_t s);
+
+// ---- layouts (rpl_layout.cu) ----
+cudaError_t launch_to_device_layout(const Handle& h, const void* src, int src_dtype, void* dst, int dst_dtype,
+                                    int64_t n0, int64_t nc, int64_t m0, int64_t mc, cudaStream_t s);
+cudaError_t launch_from_device_layout(const Handle& h, const void* src, int src_dtype, void* dst, int dst_dtype,
+                                      int64_t n0, int64_t nc, int64_t m0, int64_t mc, cudaStream_t s);
+cudaError_t launch_coef(const Handle& h, cudaStream_t s);
 
 // ---- stage kernels (rpl_stage.cu) ----
 StageParams make_params(const Handle& h, double dt, int stage);

@@ -207,7 +207,7 @@ __global__ void stress_kernel(const T* __restrict__ N, StageParams p, double rho
         for (int n = 0; n < p.Np; ++n) {
             const double cth = p.cosp[n], sth = p.sinp[n];
             for (int m = 0; m < p.Nk; ++m) {
-                const double a = (double)N[c + P * (m + p.Nk * (int64_t)n)];
+                const double a = (double)N[((int64_t)n * P + c) * p.Nk + m];
                 const double k = p.kappa[m];
                 if (a > 0.0 && k > 0.0) {
                     const double theta = p.phi[n];
@@ -226,12 +226,6 @@ __global__ void stress_kernel(const T* __restrict__ N, StageParams p, double rho
         f = (eff > 0.4 * tau_max && tau_max > 0.0) ? 0.4 * tau_max / eff : 1.0;
     }
     factor[c] = f;
-}
-
-template <typename S, typename D>
-__global__ void convert_kernel(const S* __restrict__ src, D* __restrict__ dst, int64_t n) {
-    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
-        dst[t] = (D)src[t];
 }
 
 // Neumaier compensated accumulation.
@@ -257,7 +251,7 @@ __global__ void diag_kernel(const T* __restrict__ N, int64_t Nx, int64_t Ny, int
     const double* tr = tabs + 3 * nb;
     double s0 = 0, c0 = 0, sx = 0, cx = 0, sy = 0, cy = 0, st = 0, ct = 0;
     for (int64_t b = 0; b < nb; ++b) {
-        const double a = (double)N[c + P * b];
+        const double a = (double)N[((b / Nk) * P + c) * Nk + b % Nk];  // bin b = m + Nk*n
         kadd(s0, c0, a * w[b]);
         kadd(sx, cx, a * mux[b]);
         kadd(sy, cy, a * muy[b]);
@@ -377,17 +371,6 @@ cudaError_t launch_stress_factor(const Handle& h, const void* Nin, cudaStream_t 
     else
         stress_kernel<float><<<blocks_for(P, 128), 128, 0, s>>>((const float*)Nin, p, rho_w_g, h.src.rho_air,
                                                                 h.d_wind + 3 * P);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_convert(const void* src, int src_dtype, void* dst, int dst_dtype, int64_t n, cudaStream_t s) {
-    const unsigned blocks = (unsigned)std::min<int64_t>(blocks_for(n, 256), 148 * 32);
-    if (src_dtype == RPL_F64 && dst_dtype == RPL_F32)
-        convert_kernel<double, float><<<blocks, 256, 0, s>>>((const double*)src, (float*)dst, n);
-    else if (src_dtype == RPL_F32 && dst_dtype == RPL_F64)
-        convert_kernel<float, double><<<blocks, 256, 0, s>>>((const float*)src, (double*)dst, n);
-    else
-        return cudaMemcpyAsync(dst, src, (size_t)n * (src_dtype == RPL_F64 ? 8 : 4), cudaMemcpyDeviceToDevice, s);
     return cudaGetLastError();
 }
 
