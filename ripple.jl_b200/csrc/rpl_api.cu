@@ -4,6 +4,7 @@
 
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <algorithm>
 #include <new>
@@ -196,6 +197,10 @@ int rpl_create(const rpl_desc* d, rpl_handle** out) {
     Handle* h = new (std::nothrow) Handle();
     if (!h) return fail(RPL_ERR_OOM, "host allocation failed");
     h->desc = *d;
+    {
+        const char* env = std::getenv("RPL_FORCE_COLUMN_KERNEL");
+        h->force_column_kernel = env && env[0] == '1';
+    }
     h->device = d->device;
     h->precision = d->precision;
     h->elem = elem;

@@ -86,6 +86,7 @@ struct Handle {
     double* d_diag = nullptr;      // 5 (Nx,Ny) fields + block partials
     unsigned int* d_err = nullptr;
     unsigned int* h_err = nullptr;  // pinned
+    bool force_column_kernel = false;  // RPL_FORCE_COLUMN_KERNEL=1 selects the generic FP32 column kernel
     double time = 0.0;
     int64_t iteration = 0;
     int64_t bytes = 0;
@@ -111,6 +112,11 @@ cudaError_t launch_to_device_layout(const Handle& h, const void* src, int src_dt
 cudaError_t launch_from_device_layout(const Handle& h, const void* src, int src_dtype, void* dst, int dst_dtype,
                                       int64_t n0, int64_t nc, int64_t m0, int64_t mc, cudaStream_t s);
 cudaError_t launch_coef(const Handle& h, cudaStream_t s);
+
+// ---- FP32 tiled stage kernel (rpl_tile32.cu) ----
+bool tile32_supported(const Handle& h);
+cudaError_t launch_tile32(const Handle& h, const StageParams& p, const void* Nin, const void* N0, void* Nout,
+                          cudaStream_t s);
 
 // ---- stage kernels (rpl_stage.cu) ----
 StageParams make_params(const Handle& h, double dt, int stage);

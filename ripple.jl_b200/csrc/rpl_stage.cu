@@ -442,6 +442,7 @@ StageParams make_params(const Handle& h, double dt, int stage) {
 cudaError_t launch_stage(const Handle& h, const StageParams& p, const void* Nin, const void* N0, void* Nout,
                          cudaStream_t s) {
     if (h.precision == RPL_FP64) return launch_impl<double, false>(h, p, Nin, N0, Nout, nullptr, s);
+    if (tile32_supported(h) && !h.force_column_kernel) return launch_tile32(h, p, Nin, N0, Nout, s);
     return launch_impl<float, false>(h, p, Nin, N0, Nout, nullptr, s);
 }
 

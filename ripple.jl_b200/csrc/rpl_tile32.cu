@@ -1,0 +1,358 @@
+// rpl_tile32.cu -- the FP32 stage kernel of the precision form for even Nk <= 32 with Nk % 4 == 0.
+//
+// Same arithmetic as rpl_stage.cu (wave_current_refraction.jl:74-151, intrinsic_transport.jl:14-68,
+// time_step.jl:67-105), organised for B200:
+//  * a CTA owns a TX x TY tile of horizontal cells and walks the phi ring n = 0 .. Np-1; the plane of
+//    bin n for the tile plus its 3-cell cross halo is staged in shared memory with cp.async, two
+//    planes ahead (three buffers), so x/y/kappa stencils are shared-memory reads with immediate offsets;
+//  * L = Nk_pad/2 lanes per cell, each lane holding two adjacent kappa bins as a float2, so the WENO
+//    arithmetic issues as packed FP32 pairs (FFMA2/FADD2/FMUL2, sm_100);
+//  * the phi stencil comes from a 7-deep register window of the lane's own pair; the + phi face of
+//    step n is the - face of step n+1; the face between the lane's two kappa bins and the face above
+//    them are reconstructed together, the face below comes from the lane underneath (shuffle);
+//  * reciprocals: rcp.approx of t0*t1 serves both 1/t0 and 1/t1 (t <= 1.8e19 keeps the product
+//    finite, i.e. |N| up to ~4e9), plus 1/t2 and 1/sum(alpha): three MUFU ops per face and element.
+#include <cuda_runtime.h>
+
+#include <type_traits>
+
+#include "rpl_device.cuh"
+#include "rpl_internal.h"
+
+namespace rpl {
+
+namespace {
+
+constexpr unsigned FULL = 0xffffffffu;
+constexpr int TX = 8, TY = 4;             // tile of horizontal cells per CTA
+constexpr int RW = TX + 6, RH = TY + 6;   // staged rectangle (only its cross is loaded)
+constexpr int NB = 3;                     // plane buffers
+
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, f2(-1.0f), a); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float rcpf(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float2 rcp2(float2 a) { return make_float2(rcpf(a.x), rcpf(a.y)); }
+__device__ __forceinline__ float2 sel2(bool px, bool py, float2 a, float2 b) {
+    return make_float2(px ? a.x : b.x, py ? a.y : b.y);
+}
+
+// Nonlinear part of one WENO5 face given the shared quantities of its stencil (see weno5d in
+// rpl_stage.cu): returns s2 + sum(alpha_k (v_k - s2)) / sum(alpha_k) with the weights folded
+// (0.1, 0.6, 0.3) into the candidate offsets.
+__device__ __forceinline__ float2 weno_face2(float2 d1, float2 d2, float2 d3, float2 d4, float2 D1, float2 D2,
+                                             float2 D3, float2 A1, float2 A2, float2 A3, float2 s2) {
+    const float2 g0 = fma2(f2(0.5f), D1, d2);
+    const float2 g1 = mul2(f2(0.5f), add2(d2, d3));
+    const float2 g2 = fma2(f2(-0.5f), D3, d3);
+    const float2 t0 = fma2(g0, g0, A1), t1 = fma2(g1, g1, A2), t2 = fma2(g2, g2, A3);
+    const float2 r01 = rcp2(mul2(t0, t1));
+    const float2 r0 = mul2(r01, t1), r1 = mul2(r01, t0), r2 = rcp2(t2);
+    const float2 u0 = mul2(r0, r0), u1 = mul2(r1, r1), u2 = mul2(r2, r2);
+    const float2 den = fma2(f2(0.3f), u2, fma2(f2(0.6f), u1, mul2(f2(0.1f), u0)));
+    const float2 w0 = fma2(f2(1.0f / 12.0f), d2, mul2(f2(-1.0f / 30.0f), d1));
+    const float2 w1 = fma2(f2(0.2f), d3, mul2(f2(0.1f), d2));
+    const float2 w2 = fma2(f2(0.2f), d3, mul2(f2(-0.05f), d4));
+    const float2 num = fma2(w2, u2, fma2(w1, u1, mul2(w0, u0)));
+    return fma2(num, rcp2(den), s2);
+}
+
+__device__ __forceinline__ float2 areg(float2 D) {
+    return fma2(mul2(f2(13.0f / 12.0f), D), D, f2((float)RPL_WENO_EPS));
+}
+
+// value at the face between s2 and s3 of the oriented stencil s0..s4
+__device__ __forceinline__ float2 weno5_2(float2 s0, float2 s1, float2 s2, float2 s3, float2 s4) {
+    const float2 d1 = sub2(s1, s0), d2 = sub2(s2, s1), d3 = sub2(s3, s2), d4 = sub2(s4, s3);
+    const float2 D1 = sub2(d2, d1), D2 = sub2(d3, d2), D3 = sub2(d4, d3);
+    return weno_face2(d1, d2, d3, d4, D1, D2, D3, areg(D1), areg(D2), areg(D3), s2);
+}
+
+// both faces of the cell s3 from s0..s5 oriented upwind -> downwind: lo (s2|s3), hi (s3|s4)
+__device__ __forceinline__ void weno5_pair2(float2 s0, float2 s1, float2 s2, float2 s3, float2 s4, float2 s5,
+                                            float2& lo, float2& hi) {
+    const float2 d1 = sub2(s1, s0), d2 = sub2(s2, s1), d3 = sub2(s3, s2), d4 = sub2(s4, s3), d5 = sub2(s5, s4);
+    const float2 D1 = sub2(d2, d1), D2 = sub2(d3, d2), D3 = sub2(d4, d3), D4 = sub2(d5, d4);
+    const float2 A1 = areg(D1), A2 = areg(D2), A3 = areg(D3), A4 = areg(D4);
+    lo = weno_face2(d1, d2, d3, d4, D1, D2, D3, A1, A2, A3, s2);
+    hi = weno_face2(d2, d3, d4, d5, D2, D3, D4, A2, A3, A4, s3);
+}
+
+// u * (N(+1/2) - N(-1/2)) for a periodic direction from m3..p3, upwinded per element by sign(u)
+__device__ __forceinline__ float2 flux2(float2 m3, float2 m2, float2 m1, float2 c, float2 p1, float2 p2, float2 p3,
+                                        float2 u) {
+    const bool px = u.x >= 0.0f, py = u.y >= 0.0f;
+    float2 lo, hi;
+    if (__all_sync(FULL, px && py)) {
+        weno5_pair2(m3, m2, m1, c, p1, p2, lo, hi);
+    } else if (__all_sync(FULL, !px && !py)) {
+        weno5_pair2(p3, p2, p1, c, m1, m2, lo, hi);
+    } else {
+        weno5_pair2(sel2(px, py, m3, p3), sel2(px, py, m2, p2), sel2(px, py, m1, p1), c, sel2(px, py, p1, m1),
+                    sel2(px, py, p2, m2), lo, hi);
+    }
+    // oriented upwind->downwind: positive u -> hi is +1/2; negative u -> lo is +1/2
+    const float2 diff = sub2(hi, lo);
+    return mul2(u, make_float2(px ? diff.x : -diff.x, py ? diff.y : -diff.y));
+}
+
+template <int L, bool REFRACT>
+__global__ void __launch_bounds__(TX* TY* L) tile_kernel(const float* __restrict__ Nin, const float* N0, float* Nout,
+                                                          StageParams p) {
+    constexpr int KP = 2 * L;               // kappa slots per staged column
+    constexpr int THREADS = TX * TY * L;
+    constexpr int CROSS = RW * TY + 6 * TX;  // staged columns per plane
+    extern __shared__ __align__(16) float smem[];
+    const int Nx = (int)p.Nx, Ny = (int)p.Ny, Nk = (int)p.Nk, Np = (int)p.Np;
+    const int64_t slice = (int64_t)Nx * Ny * Nk;
+    const int tiles_x = (Nx + TX - 1) / TX;
+    const int i0 = (blockIdx.x % tiles_x) * TX, j0 = (blockIdx.x / tiles_x) * TY;
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int l = tid % L;                    // lane within the cell
+    const int cell = tid / L;                 // 0 .. TX*TY-1
+    const int cx = cell % TX, cy = cell / TX;
+    const int i = i0 + cx, j = j0 + cy;
+    const bool live_cell = i < Nx && j < Ny;
+    const int ic = i < Nx ? i : Nx - 1, jc = j < Ny ? j : Ny - 1;
+    const int m0 = 2 * l;                      // this lane's kappa pair (m0, m0+1)
+    const bool live = live_cell && m0 < Nk;
+    const int mc = m0 < Nk ? m0 : Nk - 2;
+    const int64_t home = ((int64_t)jc * Nx + ic) * Nk + mc;  // offset within a slice
+
+    // cp.async chunk descriptors (16-byte chunks of the cross columns), reused for every plane
+    const int KC = Nk / 4;
+    const int nchunks = CROSS * KC;
+    constexpr int MAXC = (CROSS * 8 + THREADS - 1) / THREADS;
+    int64_t goff[MAXC];
+    int soff[MAXC];
+#pragma unroll
+    for (int k = 0; k < MAXC; ++k) {
+        const int q = tid + k * THREADS;
+        goff[k] = -1;
+        soff[k] = 0;
+        if (q < nchunks) {
+            const int col = q / KC, part = q % KC;
+            int dx, dy;
+            if (col < RW * TY) {
+                dy = col / RW;
+                dx = col % RW - 3;
+            } else {
+                const int r = col - RW * TY, yi = r / TX;
+                dx = r % TX;
+                dy = yi < 3 ? yi - 3 : TY + yi - 3;
+            }
+            int gi = i0 + dx, gj = j0 + dy;
+            gi = gi < 0 ? gi + Nx : (gi >= Nx ? gi - Nx : gi);
+            gj = gj < 0 ? gj + Ny : (gj >= Ny ? gj - Ny : gj);
+            gi = gi < 0 ? 0 : (gi >= Nx ? Nx - 1 : gi);  // tiles wider than the grid
+            gj = gj < 0 ? 0 : (gj >= Ny ? Ny - 1 : gj);
+            goff[k] = ((int64_t)gj * Nx + gi) * Nk + 4 * part;
+            soff[k] = ((dy + 3) * RW + (dx + 3)) * KP + 4 * part;
+        }
+    }
+    const int plane_floats = RW * RH * KP;
+    auto issue = [&](int n) {
+        if (n < Np) {
+            float* buf = smem + (n % NB) * plane_floats;
+            const float* src = Nin + slice * n;
+#pragma unroll
+            for (int k = 0; k < MAXC; ++k)
+                if (goff[k] >= 0) {
+                    const unsigned sa = (unsigned)__cvta_generic_to_shared(buf + soff[k]);
+                    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(src + goff[k]));
+                }
+        }
+        asm volatile("cp.async.commit_group;");
+    };
+    issue(0);
+    issue(1);
+
+    // coefficient records of the pair (FP64 -> FP32 once per ring)
+    const double* rec0 = p.coef + 8 * (((int64_t)jc * Nx + ic) * Nk + mc);
+    const double* rec1 = rec0 + 8;
+    float2 kap, Uxx, Uxy, Uyx, Uyy, Ux, Uy, cgm;
+    {
+        kap = make_float2((float)rec0[7], (float)rec1[7]);
+        Ux = make_float2((float)rec0[0], (float)rec1[0]);
+        Uy = make_float2((float)rec0[1], (float)rec1[1]);
+        Uxx = make_float2((float)rec0[2], (float)rec1[2]);
+        Uxy = make_float2((float)rec0[3], (float)rec1[3]);
+        Uyx = make_float2((float)rec0[4], (float)rec1[4]);
+        Uyy = make_float2((float)rec0[5], (float)rec1[5]);
+        cgm = make_float2((float)rec0[6], (float)rec1[6]);
+    }
+    const float2* own = reinterpret_cast<const float2*>(Nin + home);  // stride per bin: slice/2 float2
+    const int64_t s2 = slice / 2;
+    float2 w0 = f2(0.f), w1 = f2(0.f), w2 = f2(0.f), w3 = f2(0.f), w4 = f2(0.f), w5 = f2(0.f), w6 = f2(0.f);
+    if constexpr (REFRACT) {
+        auto wr = [&](int n) { return n < 0 ? n + Np : (n >= Np ? n - Np : n); };
+        w0 = own[s2 * wr(-3)]; w1 = own[s2 * wr(-2)]; w2 = own[s2 * wr(-1)]; w3 = own[0];
+        w4 = own[s2 * wr(1)]; w5 = own[s2 * wr(2)]; w6 = own[s2 * wr(3)];
+    }
+    const float dx_inv = (float)p.dx_inv, dy_inv = (float)p.dy_inv, dk_inv = (float)p.dk_inv, dp_inv = (float)p.dp_inv;
+    const float dt = (float)p.dt, ca = (float)p.a, cb = (float)p.b;
+    // kappa faces: face a between m0|m0+1 and face b between m0+1|m0+2
+    const bool ha = (m0 - 2 >= 0) && (m0 + 3 <= Nk - 1);
+    const bool hb = (m0 - 1 >= 0) && (m0 + 4 <= Nk - 1);
+    const bool hlo = (m0 - 3 >= 0) && (m0 + 2 <= Nk - 1);   // face below m0 (m0-1|m0)
+    const int kcm3 = max(m0 - 3, 0), kcm2 = max(m0 - 2, 0), kcm1 = max(m0 - 1, 0);
+    const int kcp2 = min(m0 + 2, Nk - 1), kcp3 = min(m0 + 3, Nk - 1), kcp4 = min(m0 + 4, Nk - 1);
+    const int ctr = ((cy + 3) * RW + (cx + 3)) * KP;         // this cell's column in a staged plane
+    float2 prevF = f2(0.f);
+    bool prevx = false, prevy = false, have = false;
+
+    for (int n = 0; n < Np; ++n) {
+        float2 nxt = f2(0.f);
+        if constexpr (REFRACT) nxt = own[s2 * ((n + 4) % Np)];
+        const float2 n0v = (p.stage == 1 || !live) ? f2(0.f)
+                                                    : *reinterpret_cast<const float2*>(N0 + slice * n + home);
+        asm volatile("cp.async.wait_group 1;");
+        __syncthreads();
+        issue(n + 2);
+        const float* pl = smem + (n % NB) * plane_floats + ctr;
+        // idle lanes (m0 >= Nk) read the last live pair; their results are never stored
+        auto V = [&](int dcol, int) { return *reinterpret_cast<const float2*>(pl + dcol * KP + mc); };
+        const float2 c = *reinterpret_cast<const float2*>(pl + mc);
+        // velocities (same expression order as the FP64 path)
+        const float4 tg = __ldg(p.trig32 + n);
+        const float4 g = __ldg(reinterpret_cast<const float4*>(p.cg32 + mc + Nk * n));
+        float2 ux = make_float2(g.x, g.z), uy = make_float2(g.y, g.w);
+        if (p.cg_per_cell) {
+            ux = mul2(cgm, ux);
+            uy = mul2(cgm, uy);
+        }
+        float2 G;
+        if constexpr (REFRACT) {
+            ux = add2(ux, Ux);
+            uy = add2(uy, Uy);
+            const float2 ck = mul2(mul2(f2(-1.f), kap),
+                                   add2(add2(mul2(f2(tg.x), Uxx), mul2(f2(tg.y), add2(Uyx, Uxy))), mul2(f2(tg.z), Uyy)));
+            const float2 cp = sub2(add2(mul2(f2(tg.y), sub2(Uxx, Uyy)), mul2(f2(tg.z), Uyx)), mul2(f2(tg.x), Uxy));
+            // x and y
+            const float2 fx = mul2(flux2(V(-3, m0), V(-2, m0), V(-1, m0), c, V(1, m0), V(2, m0), V(3, m0), ux), f2(dx_inv));
+            const float2 fy = mul2(flux2(V(-3 * RW, m0), V(-2 * RW, m0), V(-RW, m0), c, V(RW, m0), V(2 * RW, m0),
+                                         V(3 * RW, m0), uy), f2(dy_inv));
+            // kappa: stencil values of this lane's column (clamped like the reference)
+            const float km3 = pl[kcm3], km2 = pl[kcm2], km1 = pl[kcm1];
+            const float kp2 = pl[kcp2], kp3 = pl[kcp3], kp4 = pl[kcp4];
+            const float k0 = c.x, k1 = c.y;
+            // face a (m0|m0+1) upwinded by cell m0, face b (m0+1|m0+2) by cell m0+1
+            const bool pa = ck.x >= 0.f, pb = ck.y >= 0.f;
+            const float2 sa0 = make_float2(pa ? km2 : kp3, pb ? km1 : kp4);
+            const float2 sa1 = make_float2(pa ? km1 : kp2, pb ? k0 : kp3);
+            const float2 sa2 = make_float2(pa ? k0 : k1, pb ? k1 : kp2);
+            const float2 sa3 = make_float2(pa ? k1 : k0, pb ? kp2 : k1);
+            const float2 sa4 = make_float2(pa ? kp2 : km1, pb ? kp3 : k0);
+            float2 Fab = weno5_2(sa0, sa1, sa2, sa3, sa4);
+            Fab.x = ha ? Fab.x : (pa ? k0 : k1);
+            Fab.y = hb ? Fab.y : (pb ? k1 : kp2);
+            // the - face of cell m0+1 is face a: recompute if cell m0+1 upwinds the other way
+            float Fam1 = Fab.x;
+            if (pa != pb) {
+                const float2 t = weno5_2(make_float2(pb ? km2 : kp3, 0.f), make_float2(pb ? km1 : kp2, 0.f),
+                                         make_float2(pb ? k0 : k1, 0.f), make_float2(pb ? k1 : k0, 0.f),
+                                         make_float2(pb ? kp2 : km1, 0.f));
+                Fam1 = ha ? t.x : (pb ? k0 : k1);
+            }
+            // the - face of cell m0 is face b of the lane below (cell m0-1)
+            const float upF = __shfl_up_sync(FULL, Fab.y, 1, L);
+            const bool upP = __shfl_up_sync(FULL, (int)pb, 1, L) != 0;
+            float Flo = upF;
+            if (m0 >= 1 && upP != pa) {
+                const float2 t = weno5_2(make_float2(pa ? km3 : kp2, 0.f), make_float2(pa ? km2 : k1, 0.f),
+                                         make_float2(pa ? km1 : k0, 0.f), make_float2(pa ? k0 : km1, 0.f),
+                                         make_float2(pa ? k1 : km2, 0.f));
+                Flo = hlo ? t.x : (pa ? km1 : k0);
+            }
+            const float fk0 = ((m0 == Nk - 1) ? 0.f : ck.x * Fab.x) - ((m0 == 0) ? 0.f : ck.x * Flo);
+            const float fk1 = ((m0 + 1 == Nk - 1) ? 0.f : ck.y * Fab.y) - ck.y * Fam1;
+            const float2 fk = mul2(make_float2(fk0, fk1), f2(dk_inv));
+            // phi: window
+            const bool qx = cp.x >= 0.f, qy = cp.y >= 0.f;
+            const float2 Fpp = weno5_2(sel2(qx, qy, w1, w6), sel2(qx, qy, w2, w5), sel2(qx, qy, w3, w4),
+                                       sel2(qx, qy, w4, w3), sel2(qx, qy, w5, w2));
+            float2 Fpm = prevF;
+            if (!have || prevx != qx || prevy != qy) {
+                const float2 t = weno5_2(sel2(qx, qy, w0, w5), sel2(qx, qy, w1, w4), sel2(qx, qy, w2, w3),
+                                         sel2(qx, qy, w3, w2), sel2(qx, qy, w4, w1));
+                if (!have || prevx != qx) Fpm.x = t.x;
+                if (!have || prevy != qy) Fpm.y = t.y;
+            }
+            prevF = Fpp;
+            prevx = qx;
+            prevy = qy;
+            have = true;
+            const float2 fp = mul2(mul2(cp, sub2(Fpp, Fpm)), f2(dp_inv));
+            G = mul2(f2(-1.f), add2(add2(add2(fx, fy), fk), fp));
+        } else {
+            const float2 fx = mul2(flux2(V(-3, m0), V(-2, m0), V(-1, m0), c, V(1, m0), V(2, m0), V(3, m0), ux), f2(dx_inv));
+            const float2 fy = mul2(flux2(V(-3 * RW, m0), V(-2 * RW, m0), V(-RW, m0), c, V(RW, m0), V(2 * RW, m0),
+                                         V(3 * RW, m0), uy), f2(dy_inv));
+            G = mul2(f2(-1.f), add2(fx, fy));
+        }
+        if (p.has_wind || p.has_diss) {
+            G.x += (float)source_term(p, (int64_t)jc * Nx + ic, mc, n, (double)c.x);
+            G.y += (float)source_term(p, (int64_t)jc * Nx + ic, mc + 1, n, (double)c.y);
+        }
+        // stage update
+        float2 st = fma2(f2(dt), G, c);
+        st.x = relu(st.x);
+        st.y = relu(st.y);
+        float2 out = st;
+        if (p.stage != 1) {
+            out = fma2(f2(ca), n0v, mul2(f2(cb), st));
+            out.x = relu(out.x);
+            out.y = relu(out.y);
+        }
+        if (live) {
+            if (!isfinite(out.x) || !isfinite(out.y)) atomicOr(p.err, 1u);
+            *reinterpret_cast<float2*>(Nout + slice * n + home) = out;
+        }
+        w0 = w1; w1 = w2; w2 = w3; w3 = w4; w4 = w5; w5 = w6; w6 = nxt;
+    }
+    asm volatile("cp.async.wait_group 0;");
+}
+
+template <int L>
+cudaError_t launch_L(const Handle& h, const StageParams& p, const float* in, const float* n0, float* out,
+                     cudaStream_t s) {
+    const size_t smem = (size_t)NB * RW * RH * 2 * L * sizeof(float);
+    const int tiles = (int)(((h.desc.Nx + TX - 1) / TX) * ((h.desc.Ny + TY - 1) / TY));
+    if (p.transport == RPL_TRANSPORT_REFRACTION) {
+        auto k = tile_kernel<L, true>;
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k<<<tiles, TX * TY * L, smem, s>>>(in, n0, out, p);
+    } else {
+        auto k = tile_kernel<L, false>;
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k<<<tiles, TX * TY * L, smem, s>>>(in, n0, out, p);
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+bool tile32_supported(const Handle& h) {
+    const rpl_desc& d = h.desc;
+    return h.precision == RPL_FP32 && d.transport != RPL_TRANSPORT_NONE && d.Nk % 4 == 0 && d.Nk >= 4 &&
+           d.Nk <= 32 && (d.transport != RPL_TRANSPORT_REFRACTION || d.Np >= 3) && d.Nx >= 3 && d.Ny >= 3;
+}
+
+cudaError_t launch_tile32(const Handle& h, const StageParams& p, const void* Nin, const void* N0, void* Nout,
+                          cudaStream_t s) {
+    const int Nk = (int)h.desc.Nk;
+    const float* in = (const float*)Nin;
+    const float* n0 = (const float*)N0;
+    float* out = (float*)Nout;
+    if (Nk <= 8) return launch_L<4>(h, p, in, n0, out, s);
+    if (Nk <= 16) return launch_L<8>(h, p, in, n0, out, s);
+    return launch_L<16>(h, p, in, n0, out, s);
+}
+
+}  // namespace rpl

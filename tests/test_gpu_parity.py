@@ -189,6 +189,32 @@ def test_edge_sizes_refraction(oracle_mod, shape):
     assert rel_l2(Ng, No) <= FP64_TOL
 
 
+@pytest.mark.parametrize("column_kernel", ["0", "1"])
+@pytest.mark.parametrize("shape", [(3, 5, 4, 3), (37, 29, 8, 7), (20, 9, 24, 12), (17, 11, 32, 36)])
+def test_fp32_kernels_edge_sizes(oracle_mod, monkeypatch, shape, column_kernel):
+    """FP32 tile kernel (default) and column kernel on grids that leave partial tiles."""
+    monkeypatch.setenv("RPL_FORCE_COLUMN_KERNEL", column_kernel)
+    Nx, Ny, Nk, Np = shape
+    rng = np.random.default_rng(3 * sum(shape))
+    g = rp.RectilinearGrid(size=(Nx, Ny, 4), x=(0.0, Nx * 2.0), y=(0.0, Ny * 2.0), z=(-3.0, 0.0))
+    sg = rp.PolarWaveVectorGrid(κ=np.linspace(0.3, 0.9, Nk), φ=np.arange(Np) * 2 * math.pi / Np)
+    u = np.asfortranarray(rng.uniform(-0.3, 0.3, (Nx, Ny, 4)))
+    v = np.asfortranarray(rng.uniform(-0.3, 0.3, (Nx, Ny, 4)))
+    N0 = np.asfortranarray(rng.uniform(0.5, 1.0, shape))
+    w = workloads.Workload("edge32", g, sg, 2.0, N0, 0.05, 3, velocities={"u": u, "v": v})
+    m, Ng, No = run_both(oracle_mod, w, 3, precision="fp32")
+    assert rel_l2(Ng, No) <= FP32_TOL
+
+
+@pytest.mark.parametrize("column_kernel", ["0", "1"])
+def test_fp32_kernels_intrinsic_and_depth_field(oracle_mod, monkeypatch, column_kernel):
+    monkeypatch.setenv("RPL_FORCE_COLUMN_KERNEL", column_kernel)
+    w = workloads.seamount_eddies(N=40, Nz=8, Nk=16, Np=24, nsteps=3)
+    w.velocities = None                     # intrinsic transport with a depth field (c_g per cell)
+    m, Ng, No = run_both(oracle_mod, w, 3, precision="fp32")
+    assert rel_l2(Ng, No) <= FP32_TOL
+
+
 def test_set_get_roundtrip_and_clock():
     w = workloads.seamount_eddies(N=16, Nz=4, Nk=4, Np=6, nsteps=1)
     for precision in ("fp64", "fp32"):
