@@ -200,6 +200,8 @@ int rpl_create(const rpl_desc* d, rpl_handle** out) {
     {
         const char* env = std::getenv("RPL_FORCE_COLUMN_KERNEL");
         h->force_column_kernel = env && env[0] == '1';
+        const char* occ = std::getenv("RPL_TILE_CTAS_PER_SM");
+        h->tile_occupancy = (occ && occ[0] == '2') ? 2 : 1;
     }
     h->device = d->device;
     h->precision = d->precision;

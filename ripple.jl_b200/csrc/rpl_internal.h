@@ -87,6 +87,7 @@ struct Handle {
     unsigned int* d_err = nullptr;
     unsigned int* h_err = nullptr;  // pinned
     bool force_column_kernel = false;  // RPL_FORCE_COLUMN_KERNEL=1 selects the generic FP32 column kernel
+    int tile_occupancy = 1;            // RPL_TILE_CTAS_PER_SM=2 builds the FP32 tile kernel for 2 CTAs per SM
     double time = 0.0;
     int64_t iteration = 0;
     int64_t bytes = 0;

@@ -10,8 +10,8 @@
 //  * the phi stencil comes from a 7-deep register window of the lane's own pair; the + phi face of
 //    step n is the - face of step n+1; the face between the lane's two kappa bins and the face above
 //    them are reconstructed together, the face below comes from the lane underneath (shuffle);
-//  * reciprocals: rcp.approx of t0*t1 serves both 1/t0 and 1/t1 (t <= 1.8e19 keeps the product
-//    finite, i.e. |N| up to ~4e9), plus 1/t2 and 1/sum(alpha): three MUFU ops per face and element.
+//  * reciprocals: rcp.approx of t'^2 per indicator (finite for 4(eps+beta) <= 1.8e19, i.e. |N| up to
+//    ~2e9) and of the weight sum: four MUFU ops per face and element.
 #include <cuda_runtime.h>
 
 #include <type_traits>
@@ -44,27 +44,30 @@ __device__ __forceinline__ float2 sel2(bool px, bool py, float2 a, float2 b) {
 }
 
 // Nonlinear part of one WENO5 face given the shared quantities of its stencil (see weno5d in
-// rpl_stage.cu): returns s2 + sum(alpha_k (v_k - s2)) / sum(alpha_k) with the weights folded
-// (0.1, 0.6, 0.3) into the candidate offsets.
+// rpl_stage.cu). Every smoothness indicator is carried as 4*beta: with G0 = D1 + 2 d2, G1 = d2 + d3,
+// G2 = D3 - 2 d3 and A'_c = 4(13/12 D_c^2 + eps), t'_k = G_k^2 + A'_k = 4 (eps + beta_k) exactly as the
+// reference's indicators, scaled. The weights d_k / t_k^2 are formed as u_k = 1/t'_k^2 with the
+// linear weights (0.1, 0.6, 0.3) scaled by 10 (they and the factor 16 cancel in the normalisation):
+// returns s2 + sum(w_k u_k) / (u0 + 6 u1 + 3 u2), w_k = 10 d_k (v_k - s2).
 __device__ __forceinline__ float2 weno_face2(float2 d1, float2 d2, float2 d3, float2 d4, float2 D1, float2 D2,
                                              float2 D3, float2 A1, float2 A2, float2 A3, float2 s2) {
-    const float2 g0 = fma2(f2(0.5f), D1, d2);
-    const float2 g1 = mul2(f2(0.5f), add2(d2, d3));
-    const float2 g2 = fma2(f2(-0.5f), D3, d3);
-    const float2 t0 = fma2(g0, g0, A1), t1 = fma2(g1, g1, A2), t2 = fma2(g2, g2, A3);
-    const float2 r01 = rcp2(mul2(t0, t1));
-    const float2 r0 = mul2(r01, t1), r1 = mul2(r01, t0), r2 = rcp2(t2);
-    const float2 u0 = mul2(r0, r0), u1 = mul2(r1, r1), u2 = mul2(r2, r2);
-    const float2 den = fma2(f2(0.3f), u2, fma2(f2(0.6f), u1, mul2(f2(0.1f), u0)));
-    const float2 w0 = fma2(f2(1.0f / 12.0f), d2, mul2(f2(-1.0f / 30.0f), d1));
-    const float2 w1 = fma2(f2(0.2f), d3, mul2(f2(0.1f), d2));
-    const float2 w2 = fma2(f2(0.2f), d3, mul2(f2(-0.05f), d4));
+    const float2 G0 = fma2(f2(2.0f), d2, D1);
+    const float2 G1 = add2(d2, d3);
+    const float2 G2 = fma2(f2(-2.0f), d3, D3);
+    const float2 t0 = fma2(G0, G0, A1), t1 = fma2(G1, G1, A2), t2 = fma2(G2, G2, A3);
+    const float2 u0 = rcp2(mul2(t0, t0)), u1 = rcp2(mul2(t1, t1)), u2 = rcp2(mul2(t2, t2));
+    const float2 den = fma2(f2(3.0f), u2, fma2(f2(6.0f), u1, u0));
+    const float2 w0 = fma2(f2(5.0f / 6.0f), d2, mul2(f2(-1.0f / 3.0f), d1));
+    const float2 e3 = add2(d3, d3);
+    const float2 w1 = add2(e3, d2);
+    const float2 w2 = fma2(f2(-0.5f), d4, e3);
     const float2 num = fma2(w2, u2, fma2(w1, u1, mul2(w0, u0)));
     return fma2(num, rcp2(den), s2);
 }
 
+// A'_c = 4 (13/12 D_c^2 + eps)
 __device__ __forceinline__ float2 areg(float2 D) {
-    return fma2(mul2(f2(13.0f / 12.0f), D), D, f2((float)RPL_WENO_EPS));
+    return fma2(mul2(f2(13.0f / 3.0f), D), D, f2((float)(4.0 * RPL_WENO_EPS)));
 }
 
 // value at the face between s2 and s3 of the oriented stencil s0..s4
@@ -84,26 +87,21 @@ __device__ __forceinline__ void weno5_pair2(float2 s0, float2 s1, float2 s2, flo
     hi = weno_face2(d2, d3, d4, d5, D2, D3, D4, A2, A3, A4, s3);
 }
 
-// u * (N(+1/2) - N(-1/2)) for a periodic direction from m3..p3, upwinded per element by sign(u)
+// u * (N(+1/2) - N(-1/2)) for a periodic direction from m3..p3, upwinded per element by sign(u).
+// Branch-free (per-element selects), so the four directions' arithmetic can interleave.
 __device__ __forceinline__ float2 flux2(float2 m3, float2 m2, float2 m1, float2 c, float2 p1, float2 p2, float2 p3,
                                         float2 u) {
     const bool px = u.x >= 0.0f, py = u.y >= 0.0f;
     float2 lo, hi;
-    if (__all_sync(FULL, px && py)) {
-        weno5_pair2(m3, m2, m1, c, p1, p2, lo, hi);
-    } else if (__all_sync(FULL, !px && !py)) {
-        weno5_pair2(p3, p2, p1, c, m1, m2, lo, hi);
-    } else {
-        weno5_pair2(sel2(px, py, m3, p3), sel2(px, py, m2, p2), sel2(px, py, m1, p1), c, sel2(px, py, p1, m1),
-                    sel2(px, py, p2, m2), lo, hi);
-    }
+    weno5_pair2(sel2(px, py, m3, p3), sel2(px, py, m2, p2), sel2(px, py, m1, p1), c, sel2(px, py, p1, m1),
+                sel2(px, py, p2, m2), lo, hi);
     // oriented upwind->downwind: positive u -> hi is +1/2; negative u -> lo is +1/2
     const float2 diff = sub2(hi, lo);
     return mul2(u, make_float2(px ? diff.x : -diff.x, py ? diff.y : -diff.y));
 }
 
-template <int L, bool REFRACT>
-__global__ void __launch_bounds__(TX* TY* L) tile_kernel(const float* __restrict__ Nin, const float* N0, float* Nout,
+template <int L, bool REFRACT, int MINB>
+__global__ void __launch_bounds__(TX* TY* L, MINB) tile_kernel(const float* __restrict__ Nin, const float* N0, float* Nout,
                                                           StageParams p) {
     constexpr int KP = 2 * L;               // kappa slots per staged column
     constexpr int THREADS = TX * TY * L;
@@ -113,7 +111,7 @@ __global__ void __launch_bounds__(TX* TY* L) tile_kernel(const float* __restrict
     const int64_t slice = (int64_t)Nx * Ny * Nk;
     const int tiles_x = (Nx + TX - 1) / TX;
     const int i0 = (blockIdx.x % tiles_x) * TX, j0 = (blockIdx.x / tiles_x) * TY;
-    const int tid = threadIdx.x, lane = tid & 31;
+    const int tid = threadIdx.x;
     const int l = tid % L;                    // lane within the cell
     const int cell = tid / L;                 // 0 .. TX*TY-1
     const int cx = cell % TX, cy = cell / TX;
@@ -319,17 +317,17 @@ __global__ void __launch_bounds__(TX* TY* L) tile_kernel(const float* __restrict
     asm volatile("cp.async.wait_group 0;");
 }
 
-template <int L>
+template <int L, int MINB>
 cudaError_t launch_L(const Handle& h, const StageParams& p, const float* in, const float* n0, float* out,
                      cudaStream_t s) {
     const size_t smem = (size_t)NB * RW * RH * 2 * L * sizeof(float);
     const int tiles = (int)(((h.desc.Nx + TX - 1) / TX) * ((h.desc.Ny + TY - 1) / TY));
     if (p.transport == RPL_TRANSPORT_REFRACTION) {
-        auto k = tile_kernel<L, true>;
+        auto k = tile_kernel<L, true, MINB>;
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         k<<<tiles, TX * TY * L, smem, s>>>(in, n0, out, p);
     } else {
-        auto k = tile_kernel<L, false>;
+        auto k = tile_kernel<L, false, MINB>;
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         k<<<tiles, TX * TY * L, smem, s>>>(in, n0, out, p);
     }
@@ -350,9 +348,14 @@ cudaError_t launch_tile32(const Handle& h, const StageParams& p, const void* Nin
     const float* in = (const float*)Nin;
     const float* n0 = (const float*)N0;
     float* out = (float*)Nout;
-    if (Nk <= 8) return launch_L<4>(h, p, in, n0, out, s);
-    if (Nk <= 16) return launch_L<8>(h, p, in, n0, out, s);
-    return launch_L<16>(h, p, in, n0, out, s);
+    if (h.tile_occupancy == 2) {
+        if (Nk <= 8) return launch_L<4, 2>(h, p, in, n0, out, s);
+        if (Nk <= 16) return launch_L<8, 2>(h, p, in, n0, out, s);
+        return launch_L<16, 2>(h, p, in, n0, out, s);
+    }
+    if (Nk <= 8) return launch_L<4, 1>(h, p, in, n0, out, s);
+    if (Nk <= 16) return launch_L<8, 1>(h, p, in, n0, out, s);
+    return launch_L<16, 1>(h, p, in, n0, out, s);
 }
 
 }  // namespace rpl
