@@ -1,4 +1,5 @@
-"""Benchmark: cell-bin SSP-RK3 updates per second of the seamount-eddies workload on B200.
+"""Benchmark: cell-bin SSP-RK3 updates per second of the seamount-eddies (default) or hurricane-swell
+workload on B200.
 
 Default workload: 1024^2 grid (5 km, periodic), 32 vertical levels for the Q-transform,
 32 log-spaced kappa x 36 directions, seeded seamount depth and eddy currents, FP32
@@ -8,8 +9,11 @@ the same steps through the public API (set!, time_step!, a per-step total-action
 read, interior) with pinned host buffers. --impl reference times the reference's CPU
 path (the FP64 C++ restatement) on the host cores instead.
 
+--workload hurricane: 768^2 grid (10 km), 32 kappa x 36 directions, 4000 m depth, moving Holland
+hurricane with Janssen wind input (wave-supported stress cap) and local-saturation whitecapping.
+
 python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--precision fp32|fp64]
-               [--size 1024]
+               [--workload seamount|hurricane] [--size N]
 Under torchrun each rank advances its own copy of the workload (independent replicas).
 """
 import argparse
@@ -38,10 +42,32 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
-    ap.add_argument("--size", type=int, default=1024)
+    ap.add_argument("--workload", default="seamount", choices=["seamount", "hurricane"])
+    ap.add_argument("--size", type=int, default=0, help="grid points per side (default 1024 / 768)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    return ap.parse_args()
+    args = ap.parse_args()
+    if args.size <= 0:
+        args.size = 1024 if args.workload == "seamount" else 768
+    return args
+
+
+WORKLOAD_NAMES = {"seamount": "seamount_eddies", "hurricane": "hurricane_swell"}
+
+
+def make_workload(name, n, nsteps, n0_dtype=np.float64):
+    from ripple_b200 import workloads
+    if name == "seamount":
+        return workloads.seamount_eddies(N=n, Nz=32, Nk=32, Np=36, nsteps=nsteps, n0_dtype=n0_dtype)
+    w = workloads.hurricane_swell(N=n, Nk=32, Np=36, nsteps=nsteps)
+    if n0_dtype != np.float64:
+        w.N0 = w.N0.astype(n0_dtype, order="F")
+    return w
+
+
+def launches_per_step(name):
+    """Our kernels per RK3 step: 3 fused stage kernels; the hurricane adds 1 wind + 3 stress-cap kernels."""
+    return 3 if name == "seamount" else 7
 
 
 def peaks():
@@ -106,28 +132,33 @@ class ClockSampler:
 
 def algorithmic_bytes(w, precision):
     """Per RK3 step: 8 state words per unit (N0->N1; N1,N0->N2; N2,N0->N3) + per stage the FP64
-    per-(i,j,kappa) tables (Ux, Uy, 4 gradients, and c_g when depth varies) amortised over phi."""
+    per-(i,j,kappa) tables (Ux, Uy, 4 gradients, and c_g when depth varies) amortised over phi.
+    With a stress-capped wind source, each stage also reads its input once for the cap (one state
+    word per unit) and the per-(i,j) wind record (32 bytes, amortised over kappa and phi)."""
     s = 4 if precision == "fp32" else 8
     Nk, Np = w.spectral_grid.coordinate_size()
     c_d = 0 if np.isscalar(w.depth) or type(w.depth).__name__ == "InfiniteDepth" else 1
     tables = 3 * (6 + c_d) * 8 * (w.units // Np) if w.velocities is not None else 3 * c_d * 8 * (w.units // Np)
-    return 8 * s * w.units + tables
+    extra = 0
+    if w.sources is not None:
+        cols = w.units // (Nk * Np)
+        extra = 3 * (s * w.units + 2 * 32 * cols)
+    return 8 * s * w.units + tables + extra
 
 
-def cpu_baseline(size_hint, steps=4):
+def cpu_baseline(name, steps=4):
     """The oracle (FP64 C++ restatement of the reference CPU path, OpenMP) on a bounded sample."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
-    from ripple_b200 import workloads
     n = 128
-    w = workloads.seamount_eddies(N=n, Nz=32, Nk=32, Np=36, nsteps=steps)
+    w = make_workload(name, n, steps)
     o = oracle.Oracle(w)
     o.step(w.N0, w.dt, 1)
     t = time.perf_counter()
     o.step(w.N0, w.dt, steps)
     el = time.perf_counter() - t
     return {"value": w.units * steps / el, "unit": UNIT, "cores": oracle.num_threads(), "kind": "port",
-            "sample": f"seamount_eddies at {n}^2 x 32 kappa x 36 phi (same physics, reduced grid), "
+            "sample": f"{WORKLOAD_NAMES[name]} at {n}^2 x 32 kappa x 36 phi (same physics, reduced grid), "
                       f"{steps} RK3 steps FP64, {el:.1f} s"}
 
 
@@ -136,9 +167,8 @@ def run_reference(args, rank):
         return
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
-    from ripple_b200 import workloads
     n = 96
-    w = workloads.seamount_eddies(N=n, Nz=32, Nk=32, Np=36, nsteps=1)
+    w = make_workload(args.workload, n, 1)
     o = oracle.Oracle(w)
     N = w.N0
     for _ in range(args.warmup):
@@ -148,13 +178,13 @@ def run_reference(args, rank):
         N, _ = o.step(N, w.dt, 1)
     el = time.perf_counter() - t
     value = w.units * args.steps / el
-    sample = (f"each step one FP64 SSP-RK3 step of seamount_eddies at {n}^2 x 32 kappa x 36 phi "
-              f"(1024^2 does not fit a bounded CPU sample); per-unit throughput")
+    sample = (f"each step one FP64 SSP-RK3 step of {WORKLOAD_NAMES[args.workload]} at {n}^2 x 32 kappa x 36 phi "
+              f"({args.size}^2 does not fit a bounded CPU sample); per-unit throughput")
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
             "impl": "reference",
-            "config": {"workload": "seamount_eddies", "grid": [n, n, 32], "spectral": [32, 36],
+            "config": {"workload": WORKLOAD_NAMES[args.workload], "grid": [n, n], "spectral": [32, 36],
                        "precision": "fp64", "path": "reference CPU path restated in C++ (oracle/), OpenMP"},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": oracle.num_threads(), "kind": "port",
                              "sample": sample},
@@ -165,7 +195,7 @@ def run_reference(args, rank):
 def run_ours(args, rank, world, local_rank):
     import torch
     import ripple_b200 as rp
-    from ripple_b200 import _lib, workloads
+    from ripple_b200 import _lib
 
     torch.cuda.set_device(local_rank)
     dist = None
@@ -183,7 +213,8 @@ def run_ours(args, rank, world, local_rank):
         smi_id = "GPU-" + str(torch.cuda.get_device_properties(local_rank).uuid)
     except Exception:
         smi_id = str(local_rank)
-    w = workloads.seamount_eddies(N=args.size, Nz=32, Nk=32, Np=36, nsteps=args.steps, n0_dtype=np.float32)
+    w = make_workload(args.workload, args.size, args.steps,
+                      n0_dtype=np.float32 if args.precision == "fp32" else np.float64)
     m = w.model(args.precision, device=local_rank)
     lib, h = m._lib, m.handle
     torch_stream = torch.cuda.Stream(device=local_rank)
@@ -230,7 +261,8 @@ def run_ours(args, rank, world, local_rank):
     tp = os.path.join(ROOT, "profiles", "stage_traffic.json")
     if os.path.exists(tp):
         try:
-            traffic = json.load(open(tp)).get(f"{args.precision}_{args.size}")
+            key = f"{args.precision}_{args.size}" + ("" if args.workload == "seamount" else "_hurricane")
+            traffic = json.load(open(tp)).get(key)
         except Exception:
             traffic = None
 
@@ -263,22 +295,28 @@ def run_ours(args, rank, world, local_rank):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_baseline(args.size)
+        cpu = cpu_baseline(args.workload)
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32" if args.precision == "fp32" else "f64",
-            "data": "synthetic (seeded seamount depth, eddy currents, JONSWAP-like N0)",
-            "config": {"workload": "seamount_eddies", "grid": [args.size, args.size, 32], "spectral": [32, 36],
+            "data": ("synthetic (seeded seamount depth, eddy currents, JONSWAP-like N0)" if args.workload == "seamount"
+                     else "synthetic (Holland hurricane on a linear track, uniform N0 = 1e-6)"),
+            "config": {"workload": WORKLOAD_NAMES[args.workload], "grid": [args.size, args.size],
+                       "spectral": [32, 36],
                        "precision": args.precision, "units_per_step": w.units, "dt": dt,
                        "l2": "state (%.1f GB per buffer) larger than L2; no flush" % (w.units * (4 if args.precision == "fp32" else 8) / 1e9),
                        "parallelism": f"{world} independent replicas" if world > 1 else "1 GPU"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": traffic, "peak_kind": peak_kind, "kernel": "stage_kernel",
-                         "launch_ms": launch_ms, "algorithmic_bytes_per_launch": bytes_per_launch},
-            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": 3 * args.steps, "clocks": clocks,
+                         "traffic": traffic, "peak_kind": peak_kind,
+                         "kernel": "tile_kernel" if args.precision == "fp32" else "column_kernel",
+                         "launch_ms": launch_ms, "algorithmic_bytes_per_launch": bytes_per_launch,
+                         "launch_interval": "one RK3 stage" + ("" if args.workload == "seamount"
+                                                               else " incl. its wind/stress-cap kernels")},
+            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches_per_step(args.workload) * args.steps,
+            "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
     m.close()

@@ -71,7 +71,7 @@ cudaError_t dalloc(Handle* h, T** p, size_t count) {
 void free_all(Handle* h) {
     void* ptrs[] = {h->N, h->A, h->B, h->d_kappa, h->d_phi, h->d_cos, h->d_sin, h->d_weights, h->d_cgx,
                     h->d_cgy, h->d_cgmag, h->d_depth, h->d_coupling, h->d_wind, h->d_diag, h->d_err,
-                    h->d_coef, h->d_tab32};
+                    h->d_coef, h->d_tab32, h->d_cell32, h->d_bin32};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->h_err) cudaFreeHost(h->h_err);
@@ -200,8 +200,6 @@ int rpl_create(const rpl_desc* d, rpl_handle** out) {
     {
         const char* env = std::getenv("RPL_FORCE_COLUMN_KERNEL");
         h->force_column_kernel = env && env[0] == '1';
-        const char* occ = std::getenv("RPL_TILE_CTAS_PER_SM");
-        h->tile_occupancy = (occ && occ[0] == '2') ? 2 : 1;
     }
     h->device = d->device;
     h->precision = d->precision;
@@ -313,9 +311,11 @@ int rpl_create(const rpl_desc* d, rpl_handle** out) {
         TRY(rpl::launch_cg_field(*h, s));
     }
     TRY(dalloc(h, &h->d_coef, 8 * c3));
+    TRY(dalloc(h, &h->d_cell32, 8 * P));
+    TRY(dalloc(h, &h->d_bin32, 8 * d->Nk));
     TRY(rpl::launch_coef(*h, s));
     {
-        std::vector<float> tab32(4 * d->Np + 2 * nb);
+        std::vector<float> tab32(6 * d->Np + 3 * nb);
         for (int64_t n = 0; n < d->Np; ++n) {
             const float c = (float)cosp[n], sn = (float)sinp[n];
             tab32[4 * n] = c * c;
@@ -326,6 +326,11 @@ int rpl_create(const rpl_desc* d, rpl_handle** out) {
         for (int64_t b = 0; b < nb; ++b) {
             tab32[4 * d->Np + 2 * b] = (float)cgx[b];
             tab32[4 * d->Np + 2 * b + 1] = (float)cgy[b];
+            tab32[6 * d->Np + 2 * nb + b] = (float)tabs[b];
+        }
+        for (int64_t n = 0; n < d->Np; ++n) {
+            tab32[4 * d->Np + 2 * nb + 2 * n] = (float)cosp[n];
+            tab32[4 * d->Np + 2 * nb + 2 * n + 1] = (float)sinp[n];
         }
         TRY(dalloc(h, &h->d_tab32, tab32.size()));
         TRY(cudaMemcpyAsync(h->d_tab32, tab32.data(), tab32.size() * 4, cudaMemcpyHostToDevice, s));
@@ -467,6 +472,26 @@ int rpl_set_sources(rpl_handle* hh, const rpl_sources* src) {
     h->src.track_y = nullptr;
     h->has_sources = s.wind_kind != RPL_WIND_NONE || s.has_dissipation;
     h->wind_field_set = false;
+    // per-kappa FP32 source constants (rpl_src32.cuh)
+    {
+        const int64_t Nk = h->desc.Nk;
+        std::vector<float> bins(8 * Nk, 0.0f);
+        for (int64_t m = 0; m < Nk; ++m) {
+            const double k = h->kappa[m];
+            if (s.wind_kind != RPL_WIND_NONE) {
+                const double sw = std::sqrt(s.wind_gravity * k);
+                bins[8 * m] = (float)std::log(k);
+                bins[8 * m + 1] = (float)(k / sw);
+                bins[8 * m + 2] = (float)sw;
+            }
+            if (s.has_dissipation) {
+                const double sd = std::sqrt(s.ds_gravity * k);
+                bins[8 * m + 3] = (float)(sd * (k * k * k) / s.B_r);
+                bins[8 * m + 4] = (float)(-s.C_ds * std::pow(sd, s.sigma_power));
+            }
+        }
+        RPL_CUDA(cudaMemcpyAsync(h->d_bin32, bins.data(), bins.size() * 4, cudaMemcpyHostToDevice, h->stream));
+    }
     // factor = 1 until a stress kernel runs
     const int64_t P = h->cells;
     std::vector<double> ones(P, 1.0);

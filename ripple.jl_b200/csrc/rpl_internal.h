@@ -38,6 +38,10 @@ struct StageParams {
     const double* coef;                     // per (i,j,m) device order: 8 doubles (see rpl_layout.cu)
     const float4* trig32;                   // Np: (cos^2, cos*sin, sin^2, 0) of each direction, FP32
     const float2* cg32;                     // (Nk,Np): the cg_x, cg_y table entries rounded to FP32
+    const float2* cs32;                     // Np: (cos, sin) of each direction, FP32
+    const float* w32;                       // (Nk,Np): spectral cell measures, FP32
+    const float* cell32;                    // (Nx*Ny) records of 8 floats: wind constants (rpl_src32.cuh)
+    const float* bin32;                     // Nk records of 8 floats: per-kappa source constants
     // sources
     int has_wind, stress_cap, has_diss;
     const double* wind_U10;                 // (Nx,Ny)
@@ -46,6 +50,7 @@ struct StageParams {
     const double* stress_factor;            // (Nx,Ny)
     double rho_ratio, beta_max, z_alpha, p_in, alpha0, von_karman, wind_g;
     double C_ds, B_r, ds_p, sigma_power, ds_g;
+    float wind_K32, von_karman32, z_alpha32;  // FP32 copies: rho_ratio beta_max / kappa_vk^2, kappa_vk, z_alpha
     unsigned int* err;                      // device error word
 };
 
@@ -74,7 +79,9 @@ struct Handle {
     double* d_depth = nullptr;
     double* d_coupling = nullptr;  // 8 arrays of (Nx,Ny,Nk): Ux Uy dUxdk dUydk Uxx Uxy Uyx Uyy
     double* d_coef = nullptr;      // (Nx*Ny*Nk) records of 8 doubles in device order
-    float* d_tab32 = nullptr;      // 4*Np trig entries, then 2*Nk*Np group-velocity entries (FP32 copies)
+    float* d_tab32 = nullptr;      // FP32 copies: 4*Np trig, 2*Nk*Np group velocity, 2*Np cos/sin, Nk*Np weights
+    float* d_cell32 = nullptr;     // (Nx*Ny) x 8 floats of per-cell wind constants
+    float* d_bin32 = nullptr;      // Nk x 8 floats of per-kappa source constants
     bool currents_set = false;
     // sources
     rpl_sources src{};
@@ -87,7 +94,6 @@ struct Handle {
     unsigned int* d_err = nullptr;
     unsigned int* h_err = nullptr;  // pinned
     bool force_column_kernel = false;  // RPL_FORCE_COLUMN_KERNEL=1 selects the generic FP32 column kernel
-    int tile_occupancy = 1;            // RPL_TILE_CTAS_PER_SM=2 builds the FP32 tile kernel for 2 CTAs per SM
     double time = 0.0;
     int64_t iteration = 0;
     int64_t bytes = 0;

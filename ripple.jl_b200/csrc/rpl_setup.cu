@@ -8,6 +8,7 @@
 
 #include "rpl_device.cuh"
 #include "rpl_internal.h"
+#include "rpl_src32.cuh"
 
 namespace rpl {
 
@@ -136,6 +137,7 @@ struct WindArgs {
     int kind, rotation, drag_form;
     double speed, direction;
     double vmax, rmax, radius, shape, inflow, bx, by, cx, cy;  // cx, cy: storm centre at t
+    double alpha0, g;                                            // Charnock constant, gravity
 };
 
 __device__ __forceinline__ double friction_velocity(double U, int form) {
@@ -152,7 +154,7 @@ __device__ __forceinline__ double friction_velocity(double U, int form) {
 // pressure_correlation.jl:54-63, drag.jl:85-86).
 __global__ void wind_kernel(int64_t Nx, int64_t Ny, const double* __restrict__ xn, const double* __restrict__ yn,
                             WindArgs w, double* __restrict__ U10, double* __restrict__ theta,
-                            double* __restrict__ ustar) {
+                            double* __restrict__ ustar, float* __restrict__ cell32) {
     const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= Nx * Ny) return;
     double U = 0.0, th = 0.0;
@@ -185,9 +187,16 @@ __global__ void wind_kernel(int64_t Nx, int64_t Ny, const double* __restrict__ x
         U = U10[c];
         th = theta[c];
     }
+    const double us = friction_velocity(U, w.drag_form);
     U10[c] = U;
     theta[c] = th;
-    ustar[c] = friction_velocity(U, w.drag_form);
+    ustar[c] = us;
+    // FP32 per-cell wind constants (rpl_src32.cuh); the stress kernel fills slot 5
+    const double z1 = w.alpha0 * (us * us) / w.g;
+    const bool on = U > 0.0 && us > 0.0 && z1 > 0.0;
+    float4* rec = reinterpret_cast<float4*>(cell32 + 8 * c);
+    rec[0] = make_float4(on ? (float)us : 0.0f, on ? (float)log(z1) : 0.0f, (float)cos(th), (float)sin(th));
+    reinterpret_cast<float*>(rec + 1)[0] = on ? 1.0f : 0.0f;
 }
 
 // Wave-supported stress cap per (i,j) (precomputed_sources.jl:282-326): tau_w along the wind from
@@ -355,9 +364,52 @@ cudaError_t launch_wind(const Handle& h, double t, cudaStream_t s) {
     // xnodes / ynodes live after the wind arrays in the same allocation
     const double* xn = h.d_wind + 4 * P;
     const double* yn = xn + d.Nx;
+    w.alpha0 = h.src.alpha0;
+    w.g = h.src.wind_gravity;
     wind_kernel<<<blocks_for(P, 256), 256, 0, s>>>(d.Nx, d.Ny, xn, yn, w, h.d_wind, h.d_wind + P,
-                                                    h.d_wind + 2 * P);
+                                                    h.d_wind + 2 * P, h.d_cell32);
     return cudaGetLastError();
+}
+
+// FP32 form of stress_kernel: one warp per (i,j), lane m over kappa bins m, m+32, ...; each lane sums
+// its bins over the direction ring in FP32, then the warp reduces. Writes the factor to the FP32 cell
+// record (slot 5) and to the FP64 factor field.
+__global__ void stress32_kernel(const float* __restrict__ N, StageParams p, float rho_w_g, float rho_air,
+                                float* cell32, double* __restrict__ factor) {
+    const int64_t c = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    const int64_t P = p.Nx * p.Ny;
+    if (c >= P) return;  // uniform per warp
+    const float* r = cell32 + 8 * c;
+    const Cell32 q{r[0], r[1], r[2], r[3], r[4], 1.0f, 0.0f, 0.0f};
+    float f = 1.0f;
+    if (q.on > 0.5f) {
+        float twx = 0.0f, twy = 0.0f;
+        for (int m = lane; m < (int)p.Nk; m += 32) {
+            const Bin32 b = load_bin32(p.bin32 + 8 * m);
+            for (int n = 0; n < (int)p.Np; ++n) {
+                const float2 cs = __ldg(p.cs32 + n);
+                const float a = __ldg(N + ((int64_t)n * P + c) * p.Nk + m);
+                float cos_tu;
+                const float rate = wind_rate32(p, q, b, cs.x, cs.y, cos_tu);
+                const float mf = a > 0.0f ? rate * a * b.invC * __ldg(p.w32 + m + p.Nk * n) : 0.0f;
+                twx = fmaf(mf, cs.x, twx);
+                twy = fmaf(mf, cs.y, twy);
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            twx += __shfl_xor_sync(0xffffffffu, twx, o);
+            twy += __shfl_xor_sync(0xffffffffu, twy, o);
+        }
+        const float par = fmaf(twx, q.cu, twy * q.su) * rho_w_g;
+        const float tau_max = rho_air * (q.ustar * q.ustar);
+        const float eff = fmaxf(par, 0.0f);
+        f = (eff > 0.4f * tau_max && tau_max > 0.0f) ? 0.4f * tau_max / eff : 1.0f;
+    }
+    if (lane == 0) {
+        cell32[8 * c + 5] = f;
+        factor[c] = (double)f;
+    }
 }
 
 cudaError_t launch_stress_factor(const Handle& h, const void* Nin, cudaStream_t s) {
@@ -369,8 +421,8 @@ cudaError_t launch_stress_factor(const Handle& h, const void* Nin, cudaStream_t 
         stress_kernel<double><<<blocks_for(P, 128), 128, 0, s>>>((const double*)Nin, p, rho_w_g, h.src.rho_air,
                                                                  h.d_wind + 3 * P);
     else
-        stress_kernel<float><<<blocks_for(P, 128), 128, 0, s>>>((const float*)Nin, p, rho_w_g, h.src.rho_air,
-                                                                h.d_wind + 3 * P);
+        stress32_kernel<<<blocks_for(P * 32, 256), 256, 0, s>>>((const float*)Nin, p, (float)rho_w_g,
+                                                                (float)h.src.rho_air, h.d_cell32, h.d_wind + 3 * P);
     return cudaGetLastError();
 }
 

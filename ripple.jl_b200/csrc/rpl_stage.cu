@@ -422,6 +422,10 @@ StageParams make_params(const Handle& h, double dt, int stage) {
     p.coef = h.d_coef;
     p.trig32 = reinterpret_cast<const float4*>(h.d_tab32);
     p.cg32 = reinterpret_cast<const float2*>(h.d_tab32 + 4 * d.Np);
+    p.cs32 = reinterpret_cast<const float2*>(h.d_tab32 + 4 * d.Np + 2 * d.Nk * d.Np);
+    p.w32 = h.d_tab32 + 6 * d.Np + 2 * d.Nk * d.Np;
+    p.cell32 = h.d_cell32;
+    p.bin32 = h.d_bin32;
     p.has_wind = h.has_sources && h.src.wind_kind != RPL_WIND_NONE;
     p.stress_cap = h.has_sources && h.src.stress_cap;
     p.has_diss = h.has_sources && h.src.has_dissipation;
@@ -435,6 +439,9 @@ StageParams make_params(const Handle& h, double dt, int stage) {
     p.alpha0 = h.src.alpha0; p.von_karman = h.src.von_karman; p.wind_g = h.src.wind_gravity;
     p.C_ds = h.src.C_ds; p.B_r = h.src.B_r; p.ds_p = h.src.ds_p; p.sigma_power = h.src.sigma_power;
     p.ds_g = h.src.ds_gravity;
+    p.wind_K32 = p.has_wind ? (float)(p.rho_ratio * (p.beta_max / (p.von_karman * p.von_karman))) : 0.0f;
+    p.von_karman32 = (float)p.von_karman;
+    p.z_alpha32 = (float)p.z_alpha;
     p.err = h.d_err;
     return p;
 }

@@ -18,6 +18,7 @@
 
 #include "rpl_device.cuh"
 #include "rpl_internal.h"
+#include "rpl_src32.cuh"
 
 namespace rpl {
 
@@ -100,8 +101,8 @@ __device__ __forceinline__ float2 flux2(float2 m3, float2 m2, float2 m1, float2 
     return mul2(u, make_float2(px ? diff.x : -diff.x, py ? diff.y : -diff.y));
 }
 
-template <int L, bool REFRACT, int MINB>
-__global__ void __launch_bounds__(TX* TY* L, MINB) tile_kernel(const float* __restrict__ Nin, const float* N0, float* Nout,
+template <int L, bool REFRACT, bool SRC>
+__global__ void __launch_bounds__(TX* TY* L, 1) tile_kernel(const float* __restrict__ Nin, const float* N0, float* Nout,
                                                           StageParams p) {
     constexpr int KP = 2 * L;               // kappa slots per staged column
     constexpr int THREADS = TX * TY * L;
@@ -204,6 +205,14 @@ __global__ void __launch_bounds__(TX* TY* L, MINB) tile_kernel(const float* __re
     const int ctr = ((cy + 3) * RW + (cx + 3)) * KP;         // this cell's column in a staged plane
     float2 prevF = f2(0.f);
     bool prevx = false, prevy = false, have = false;
+    // source constants of this cell and of the lane's two kappa bins
+    Cell32 wc{};
+    Bin32 wb0{}, wb1{};
+    if constexpr (SRC) {
+        wc = load_cell32(p.cell32 + 8 * ((int64_t)jc * Nx + ic));
+        wb0 = load_bin32(p.bin32 + 8 * mc);
+        wb1 = load_bin32(p.bin32 + 8 * (mc + 1));
+    }
 
     for (int n = 0; n < Np; ++n) {
         float2 nxt = f2(0.f);
@@ -294,9 +303,10 @@ __global__ void __launch_bounds__(TX* TY* L, MINB) tile_kernel(const float* __re
                                          V(3 * RW, m0), uy), f2(dy_inv));
             G = mul2(f2(-1.f), add2(fx, fy));
         }
-        if (p.has_wind || p.has_diss) {
-            G.x += (float)source_term(p, (int64_t)jc * Nx + ic, mc, n, (double)c.x);
-            G.y += (float)source_term(p, (int64_t)jc * Nx + ic, mc + 1, n, (double)c.y);
+        if constexpr (SRC) {
+            const float2 cs = __ldg(p.cs32 + n);
+            G.x += source32(p, wc, wb0, cs.x, cs.y, c.x);
+            G.y += source32(p, wc, wb1, cs.x, cs.y, c.y);
         }
         // stage update
         float2 st = fma2(f2(dt), G, c);
@@ -317,21 +327,26 @@ __global__ void __launch_bounds__(TX* TY* L, MINB) tile_kernel(const float* __re
     asm volatile("cp.async.wait_group 0;");
 }
 
-template <int L, int MINB>
+template <int L, bool REFRACT, bool SRC>
+cudaError_t launch_variant(const StageParams& p, const float* in, const float* n0, float* out, int tiles,
+                           cudaStream_t s) {
+    const size_t smem = (size_t)NB * RW * RH * 2 * L * sizeof(float);
+    auto k = tile_kernel<L, REFRACT, SRC>;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k<<<tiles, TX * TY * L, smem, s>>>(in, n0, out, p);
+    return cudaGetLastError();
+}
+
+template <int L>
 cudaError_t launch_L(const Handle& h, const StageParams& p, const float* in, const float* n0, float* out,
                      cudaStream_t s) {
-    const size_t smem = (size_t)NB * RW * RH * 2 * L * sizeof(float);
     const int tiles = (int)(((h.desc.Nx + TX - 1) / TX) * ((h.desc.Ny + TY - 1) / TY));
-    if (p.transport == RPL_TRANSPORT_REFRACTION) {
-        auto k = tile_kernel<L, true, MINB>;
-        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k<<<tiles, TX * TY * L, smem, s>>>(in, n0, out, p);
-    } else {
-        auto k = tile_kernel<L, false, MINB>;
-        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k<<<tiles, TX * TY * L, smem, s>>>(in, n0, out, p);
-    }
-    return cudaGetLastError();
+    const bool refract = p.transport == RPL_TRANSPORT_REFRACTION;
+    const bool src = p.has_wind || p.has_diss;
+    if (refract) return src ? launch_variant<L, true, true>(p, in, n0, out, tiles, s)
+                            : launch_variant<L, true, false>(p, in, n0, out, tiles, s);
+    return src ? launch_variant<L, false, true>(p, in, n0, out, tiles, s)
+               : launch_variant<L, false, false>(p, in, n0, out, tiles, s);
 }
 
 }  // namespace
@@ -348,14 +363,9 @@ cudaError_t launch_tile32(const Handle& h, const StageParams& p, const void* Nin
     const float* in = (const float*)Nin;
     const float* n0 = (const float*)N0;
     float* out = (float*)Nout;
-    if (h.tile_occupancy == 2) {
-        if (Nk <= 8) return launch_L<4, 2>(h, p, in, n0, out, s);
-        if (Nk <= 16) return launch_L<8, 2>(h, p, in, n0, out, s);
-        return launch_L<16, 2>(h, p, in, n0, out, s);
-    }
-    if (Nk <= 8) return launch_L<4, 1>(h, p, in, n0, out, s);
-    if (Nk <= 16) return launch_L<8, 1>(h, p, in, n0, out, s);
-    return launch_L<16, 1>(h, p, in, n0, out, s);
+    if (Nk <= 8) return launch_L<4>(h, p, in, n0, out, s);
+    if (Nk <= 16) return launch_L<8>(h, p, in, n0, out, s);
+    return launch_L<16>(h, p, in, n0, out, s);
 }
 
 }  // namespace rpl

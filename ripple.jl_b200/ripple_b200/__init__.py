@@ -11,7 +11,7 @@ from .sources import (BulkWindDrag, Clockwise, Counterclockwise, HollandHurrican
                       LocalSaturationDissipation, PrecomputedSources, PressureCorrelationInput)
 from .model import (Clock, ProductField, Simulation, SpectralWaveModel, WENO, WaveActionField,
                     compute_tendencies, interior, run_, set_, time_step)
-from .diagnostics import (diagnostics, m0, mean_direction, root_mean_square_wavenumber,
+from .diagnostics import (diagnostics, m0, mean_direction, mean_period, root_mean_square_wavenumber,
                           significant_wave_height, total_action)
 
 __all__ = [n for n in dir() if not n.startswith("_")]

@@ -44,3 +44,25 @@ def mean_direction(N):
 
 def total_action(N):
     return diagnostics(N)["total_action"]
+
+
+def mean_period(N, gravity=9.81):
+    """Mean wave period per (i,j), T = 2 pi m0 / m_sigma with m_sigma = sum N sigma(kappa, d) w over the
+    spectral cells, sigma = sqrt(g kappa tanh(kappa d)) (deep water when d is infinite). The reference
+    defines mean_period only on frequency-direction grids (src/Diagnostics/moments.jl:362-370); this is
+    its analogue on the polar wavenumber grid, computed on the host from the interior (FP64)."""
+    m = _model_of(N)
+    A = np.asarray(N.interior(), dtype=np.float64)             # (Nx, Ny, Nk, Np)
+    sg = m.spectral_grid
+    w = np.asarray(sg.weights, dtype=np.float64)               # (Nk, Np)
+    k = np.asarray(sg.kappa, dtype=np.float64)
+    d = m.depth_values()                                       # scalar, inf or (Nx, Ny)
+    if np.isscalar(d):
+        sig = np.sqrt(gravity * k * (np.tanh(k * d) if np.isfinite(d) else 1.0))
+        m_s = np.einsum("ijmn,mn->ij", A, w * sig[:, None])
+    else:
+        sig = np.sqrt(gravity * k[None, None, :] * np.tanh(k[None, None, :] * np.asarray(d)[:, :, None]))
+        m_s = np.einsum("ijmn,mn,ijm->ij", A, w, sig)
+    m0v = np.einsum("ijmn,mn->ij", A, w)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        return np.where(m_s > 0, 2.0 * np.pi * m0v / m_s, 0.0)

@@ -319,6 +319,14 @@ class SpectralWaveModel:
                                          dptr(self._u), dptr(self._v), 1e-6))
         self._q = dict(zfaces=zf, kind=qkind, const=qconst, field=qfield)
 
+    def depth_values(self):
+        """The model depth as a scalar (math.inf for InfiniteDepth) or an (Nx, Ny) array."""
+        if self._depth_kind == _lib.RPL_DEPTH_INFINITE:
+            return math.inf
+        if self._depth_kind == _lib.RPL_DEPTH_CONSTANT:
+            return self._depth_const
+        return np.asarray(self._depth_field).reshape((self.grid.Nx, self.grid.Ny), order="F")
+
     def coupling_fields(self):
         """Ux, Uy, dUx/dkappa, dUy/dkappa, Ux_x, Ux_y, Uy_x, Uy_y as (Nx, Ny, Nk) arrays."""
         Nk = self.spectral_grid.coordinate_size()[0]

@@ -111,6 +111,24 @@ def test_hurricane_sources_reduced(oracle_mod, precision, tol):
     assert np.max(np.abs(Ng - No)) > 0 or precision == "fp64"
 
 
+@pytest.mark.parametrize("column_kernel", ["0", "1"])
+def test_hurricane_fp32_sources_both_kernels(oracle_mod, monkeypatch, column_kernel):
+    """FP32 source path (tile kernel: per-cell/per-kappa FP32 constants and the warp-per-column FP32
+    stress cap; column kernel: FP64 per-unit sources) on a ragged action field with the cap active.
+    Three steps: from this random start the wind input grows the action by up to ~e^1.3 per step, a
+    stiff regime in which rounding differences grow (after 12 steps FP32 and FP64 runs differ by
+    ~1e-3 rel-L2 with either source path)."""
+    monkeypatch.setenv("RPL_FORCE_COLUMN_KERNEL", column_kernel)
+    w = workloads.hurricane_swell(N=48, Nk=32, Np=36, nsteps=3)
+    rng = np.random.default_rng(11)
+    w.N0 = np.asfortranarray(rng.uniform(0.5e-6, 1.5e-6, w.N0.shape))
+    f = oracle_mod.Oracle(w).stress_factor(w.N0)
+    assert np.min(f) < 0.5 and np.mean(f < 1.0) > 0.05      # the cap binds in part of the domain
+    m, Ng, No = run_both(oracle_mod, w, 3, precision="fp32")
+    assert rel_l2(Ng, No) <= FP32_TOL
+    assert np.max(np.abs(Ng - No)) > 0
+
+
 def test_stress_factor_and_wind_match_oracle(oracle_mod):
     w = workloads.hurricane_swell(N=24, Nk=16, Np=24, nsteps=2)
     rng = np.random.default_rng(5)
