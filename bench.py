@@ -42,7 +42,11 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
-    ap.add_argument("--workload", default="seamount", choices=["seamount", "hurricane"])
+    ap.add_argument("--workload", default="seamount", choices=["seamount", "hurricane", "ensemble"])
+    ap.add_argument("--members", type=int, default=64, help="ensemble members (--workload ensemble)")
+    ap.add_argument("--autotune-cache", default="", help="tile-shape cache file (--workload ensemble)")
+    ap.add_argument("--member-sizes", default="64,128,256,384",
+                    help="grid sizes the ensemble members are drawn from (--workload ensemble)")
     ap.add_argument("--size", type=int, default=0, help="grid points per side (default 1024 / 768)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -52,11 +56,15 @@ def parse():
     return args
 
 
-WORKLOAD_NAMES = {"seamount": "seamount_eddies", "hurricane": "hurricane_swell"}
+WORKLOAD_NAMES = {"seamount": "seamount_eddies", "hurricane": "hurricane_swell", "ensemble": "ensemble_members"}
 
 
 def make_workload(name, n, nsteps, n0_dtype=np.float64):
     from ripple_b200 import workloads
+    if name == "ensemble":
+        # the CPU sample of the ensemble: its 32 kappa x 36 direction physics on an n^2 member grid
+        return workloads.seamount_eddies(N=n, Nz=16, Nk=32, Np=36, nsteps=nsteps, seed=4, L=n * 5000.0,
+                                         n0_dtype=n0_dtype)
     if name == "seamount":
         return workloads.seamount_eddies(N=n, Nz=32, Nk=32, Np=36, nsteps=nsteps, n0_dtype=n0_dtype)
     w = workloads.hurricane_swell(N=n, Nk=32, Np=36, nsteps=nsteps)
@@ -146,11 +154,10 @@ def algorithmic_bytes(w, precision):
     return 8 * s * w.units + tables + extra
 
 
-def cpu_baseline(name, steps=4):
+def cpu_baseline(name, steps=4, n=128):
     """The oracle (FP64 C++ restatement of the reference CPU path, OpenMP) on a bounded sample."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
-    n = 128
     w = make_workload(name, n, steps)
     o = oracle.Oracle(w)
     o.step(w.N0, w.dt, 1)
@@ -325,6 +332,143 @@ def run_ours(args, rank, world, local_rank):
         dist.destroy_process_group()
 
 
+def run_ensemble(args, rank, world, local_rank):
+    """The batching form: `--members` seeded members of uneven grids, one persistent launch per stage,
+    one CUDA graph per RK3 step; timed beside the same steps as per-member sequential launches."""
+    import torch
+    import ripple_b200 as rp
+    from ripple_b200 import _lib, workloads
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    try:
+        smi_id = "GPU-" + str(torch.cuda.get_device_properties(local_rank).uuid)
+    except Exception:
+        smi_id = str(local_rank)
+    models, dts, nbytes_alg, shapes_info = [], [], 0.0, []
+    t_build = time.perf_counter()
+    sizes = tuple(int(x) for x in args.member_sizes.split(","))
+    for w in workloads.ensemble_members(count=args.members, seed=4, nsteps=args.steps, sizes=sizes):
+        m = w.model("fp32", device=local_rank)
+        models.append(m)
+        dts.append(w.dt)
+        nbytes_alg += algorithmic_bytes(w, "fp32")
+        shapes_info.append((w.grid.Nx, w.spectral_grid.coordinate_size()))
+        w.N0 = None
+    t_build = time.perf_counter() - t_build
+    cache = args.autotune_cache or None
+    t_tune = time.perf_counter()
+    ens = rp.Ensemble(models, dts, use_graph=True, autotune=True, autotune_cache=cache)
+    t_tune = time.perf_counter() - t_tune
+    lib, h = ens._lib, ens.handle
+    units = ens.units
+    stream = torch.cuda.Stream(device=local_rank)
+    _lib.check(lib.rpl_ensemble_set_stream(h, _lib.ctypes.c_void_p(stream.cuda_stream)))
+
+    def timed(step_fn, k):
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier()
+        with torch.cuda.stream(stream):
+            start.record(stream)
+            _lib.check(step_fn(h, k))
+            end.record(stream)
+        stream.synchronize()
+        _lib.check(lib.rpl_ensemble_sync(h))
+        barrier()
+        ms = start.elapsed_time(end)
+        if dist is not None:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    _lib.check(lib.rpl_ensemble_step_async(h, args.warmup))
+    _lib.check(lib.rpl_ensemble_sync(h))
+    with ClockSampler(smi_id) as clk:
+        ms = timed(lib.rpl_ensemble_step_async, args.steps)
+    clocks = clk.summary()
+    _lib.check(lib.rpl_ensemble_step_sequential_async(h, args.warmup))
+    _lib.check(lib.rpl_ensemble_sync(h))
+    ms_seq = timed(lib.rpl_ensemble_step_sequential_async, args.steps)
+    value = world * units * args.steps / (ms / 1e3)
+    peak, peak_kind = peaks()
+    launch_ms = ms / args.steps / 3.0
+    achieved = nbytes_alg / 3.0 / (launch_ms / 1e3) / 1e9
+
+    e2e = None
+    if not args.no_e2e:
+        # one pinned buffer holding every member's state back to back (filled untimed from the devices)
+        host = torch.empty(units, dtype=torch.float32, pin_memory=True)
+        offs = np.cumsum([0] + [int(np.prod(m.action.size)) for m in models])
+        ptr = lambda i: _lib.ctypes.c_void_p(host.data_ptr() + 4 * int(offs[i]))
+        for i, m in enumerate(models):
+            _lib.check(m._lib.rpl_get_action(m.handle, ptr(i), _lib.RPL_F32, 0))
+        tot = np.zeros(1)
+        barrier()
+        t0 = time.perf_counter()
+        for i, m in enumerate(models):       # every member's state from pinned host memory
+            _lib.check(m._lib.rpl_set_action(m.handle, ptr(i), _lib.RPL_F32, 0))
+        for _ in range(args.steps):
+            _lib.check(lib.rpl_ensemble_step(h, 1))
+            for m in models:
+                _lib.check(m._lib.rpl_diagnostics(m.handle, None, None, None, None, _lib.dptr(tot)))
+        for i, m in enumerate(models):
+            _lib.check(m._lib.rpl_get_action(m.handle, ptr(i), _lib.RPL_F32, 0))
+        el = time.perf_counter() - t0
+        if dist is not None:
+            t = torch.tensor([el], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            el = float(t.item())
+        e2e = {"value": world * units * args.steps / el, "unit": UNIT,
+               "h2d_bytes_per_step": 4 * units / args.steps,
+               "d2h_bytes_per_step": (4 * units + 8 * len(models) * args.steps) / args.steps,
+               "includes": "set! of every member from pinned host, K x (ensemble step + per-member total_action "
+                           "read), interior of every member to pinned host"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline("ensemble", steps=20, n=64)
+    if rank == 0:
+        classes = {}
+        for (N, (Nk, Np)), shp in zip(shapes_info, ens.shapes()):
+            classes.setdefault(f"{N}^2x{Nk}x{Np}", [0, shp])[0] += 1
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded members: seamount depth, vortex or eddy currents U0 0.1-0.8 m/s, JONSWAP N0)",
+            "config": {"workload": "ensemble_members", "members": len(models), "seed": 4, "member_sizes": sizes,
+                       "units_per_step": units, "classes": {k: {"count": v[0], "tile": v[1]} for k, v in classes.items()},
+                       "sequential_ms_per_step": ms_seq / args.steps,
+                       "speedup_vs_sequential": ms_seq / ms,
+                       "build_s": t_build, "autotune_s": t_tune,
+                       "l2": "state (%.1f GB per buffer set) larger than L2; no flush" % (4 * units / 1e9),
+                       "parallelism": f"{world} independent replicas" if world > 1 else "1 GPU"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": None, "peak_kind": peak_kind, "kernel": "ensemble_kernel",
+                         "launch_ms": launch_ms, "algorithmic_bytes_per_launch": nbytes_alg / 3.0,
+                         "launch_interval": "one RK3 stage of every member (graph replay: counter reset + 3 launches per step)"},
+            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": 3 * args.steps, "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    ens.close()
+    for m in models:
+        m.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -332,6 +476,9 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank)
+        return
+    if args.workload == "ensemble":
+        run_ensemble(args, rank, world, local_rank)
         return
     run_ours(args, rank, world, local_rank)
 

@@ -193,6 +193,46 @@ int rpl_diagnostics_static(const void* N, int32_t dtype, int64_t Nx, int64_t Ny,
                            const double* measures, double dx, double dy, double* m0, double* hs,
                            double* krms, double* mean_dir, double* total, void* stream);
 
+/* ---- Ensemble (batching form) ----
+ * No counterpart in the reference, which advances one model per time_step! call (time_step.jl:119-170);
+ * a Julia caller would otherwise loop time_step! over its members. An ensemble advances many
+ * independent FP32 models ("members", each made by rpl_create and set up as usual: currents, action)
+ * by one SSP-RK3 step each with three launches in total: per stage one persistent kernel whose CTAs
+ * take (member, tile) work items from an atomic counter. One step (counter reset + three launches)
+ * is captured once in a CUDA graph and replayed. Members must be FP32, on one device, share one
+ * transport kind (refraction or intrinsic), have no sources, 4 <= Nk <= 32 with Nk % 4 == 0 and
+ * Nx, Ny >= 3. Each member keeps its own dt; every step advances every member's clock by its dt.
+ * The tile shape of each size class (Nx, Ny, Nk, Np, transport, depth kind) comes from the autotuner
+ * (rpl_ensemble_autotune) or, untuned, a default per Nk. */
+typedef struct rpl_ensemble rpl_ensemble;
+
+typedef struct rpl_ensemble_options {
+    int32_t abi_version;          /* RPL_ABI_VERSION */
+    int32_t use_graph;            /* 1: replay one captured CUDA graph per step; 0: three launches */
+    int32_t autotune;             /* 1: tune size classes missing from the cache during creation */
+    int32_t reserved;
+    const char* autotune_cache;   /* text file of tuned shapes, read at creation and appended to by
+                                     the autotuner; NULL: no file */
+} rpl_ensemble_options;
+
+int rpl_ensemble_create(rpl_handle* const* members, const double* dt, int32_t count,
+                        const rpl_ensemble_options* options, rpl_ensemble** out);
+int rpl_ensemble_destroy(rpl_ensemble* e);
+/* nsteps RK3 steps of every member; returns after the work drained and every member's error word was
+ * checked. The _async form only enqueues (the members' streams wait for it); rpl_ensemble_sync checks. */
+int rpl_ensemble_step(rpl_ensemble* e, int64_t nsteps);
+int rpl_ensemble_step_async(rpl_ensemble* e, int64_t nsteps);
+/* The baseline: the same steps as per-member sequential launches of the single-model kernels. */
+int rpl_ensemble_step_sequential_async(rpl_ensemble* e, int64_t nsteps);
+int rpl_ensemble_sync(rpl_ensemble* e);
+/* Times every candidate tile shape of each size class (stage-1 launches into the members' scratch
+ * buffers, the state is not changed) and keeps the fastest; force = 0 keeps shapes found in the cache. */
+int rpl_ensemble_autotune(rpl_ensemble* e, int32_t force);
+/* Tile shape used for member i: kappa-pair lanes per cell, tile width and height in cells. */
+int rpl_ensemble_shape(const rpl_ensemble* e, int32_t member, int32_t* lanes, int32_t* tile_x, int32_t* tile_y);
+/* Run on the caller's CUDA stream (cudaStream_t on the members' device); invalidates the graph. */
+int rpl_ensemble_set_stream(rpl_ensemble* e, void* stream);
+
 /* Device bytes held by the handle. */
 int rpl_device_bytes(rpl_handle* h, int64_t* bytes);
 /* Thread-local message of the last failing call on this thread ("" if none). */

@@ -54,6 +54,38 @@ struct StageParams {
     unsigned int* err;                      // device error word
 };
 
+// Arguments of one FP32 tile-kernel stage launch over one model (rpl_tile32.cu): the buffers and the
+// FP32 view of StageParams that the tile body reads. Plain words only (copied to shared memory by the
+// ensemble kernel).
+struct TileArgs {
+    const float* Nin;
+    const float* N0;
+    float* Nout;
+    const double* coef;
+    const float4* trig32;
+    const float2* cg32;
+    const float2* cs32;
+    const float* cell32;
+    const float* bin32;
+    unsigned int* err;
+    int Nx, Ny, Nk, Np, stage, cg_per_cell, has_wind, stress_cap, has_diss, pad0;
+    float dx_inv, dy_inv, dk_inv, dp_inv, dt, a, b;
+    float wind_K32, von_karman32, z_alpha32, p_in, ds_p;
+    float pad1, pad2;
+};
+
+// Tile shapes (kappa-pair lanes per cell L, tile TX x TY) compiled into the ensemble kernel; every
+// shape has TX*TY*L = ENSEMBLE_THREADS threads. The autotuner picks one per size class.
+struct TileShape {
+    int L, TX, TY;
+};
+constexpr int ENSEMBLE_THREADS = 512;
+constexpr int kNumEnsembleShapes = 9;
+constexpr TileShape kEnsembleShapes[kNumEnsembleShapes] = {
+    {16, 8, 4}, {16, 4, 8}, {16, 16, 2},   // Nk 17..32
+    {8, 8, 8},  {8, 16, 4}, {8, 4, 16},    // Nk 9..16
+    {4, 16, 8}, {4, 8, 16}, {4, 32, 4}};   // Nk 4..8
+
 struct Handle {
     rpl_desc desc{};
     std::vector<double> xnodes, ynodes, kappa, kappa_faces, phi, phi_faces, depth_field, weights;
@@ -124,6 +156,14 @@ cudaError_t launch_coef(const Handle& h, cudaStream_t s);
 bool tile32_supported(const Handle& h);
 cudaError_t launch_tile32(const Handle& h, const StageParams& p, const void* Nin, const void* N0, void* Nout,
                           cudaStream_t s);
+int tile_lanes(int64_t Nk);                       // L used for Nk: 4, 8 or 16
+size_t tile_smem_bytes(int L, int TX, int TY);
+TileArgs make_tile_args(const Handle& h, const StageParams& p, const void* Nin, const void* N0, void* Nout);
+cudaError_t prepare_ensemble_kernels();           // shared-memory attribute, once per device
+size_t ensemble_smem_bytes();
+int ensemble_grid(bool refract, int device);      // resident CTAs: SMs x CTAs per SM
+cudaError_t launch_ensemble_stage(bool refract, const TileArgs* d_args, const int4* d_items, int nitems,
+                                  unsigned int* d_counter, int grid, cudaStream_t s);
 
 // ---- stage kernels (rpl_stage.cu) ----
 StageParams make_params(const Handle& h, double dt, int stage);

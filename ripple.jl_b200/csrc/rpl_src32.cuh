@@ -37,7 +37,8 @@ __device__ __forceinline__ Bin32 load_bin32(const float* rec) {
 __device__ __forceinline__ float pow_pos32(float x, float e) { return exp2f(e * log2f(x)); }
 
 // Raw Janssen growth rate of one bin (direction cos/sin cth, sth), 0 outside the growth window.
-__device__ __forceinline__ float wind_rate32(const StageParams& p, const Cell32& c, const Bin32& b, float cth,
+template <class P>
+__device__ __forceinline__ float wind_rate32(const P& p, const Cell32& c, const Bin32& b, float cth,
                                              float sth, float& cos_tu) {
     cos_tu = fmaf(cth, c.cu, sth * c.su);
     const float inv_age = fmaf(c.ustar, b.invC, p.z_alpha32);
@@ -51,7 +52,8 @@ __device__ __forceinline__ float wind_rate32(const StageParams& p, const Cell32&
 }
 
 // Source tendency of one cell-bin with action a: wind growth (stress-capped) minus whitecapping.
-__device__ __forceinline__ float source32(const StageParams& p, const Cell32& c, const Bin32& b, float cth, float sth,
+template <class P>
+__device__ __forceinline__ float source32(const P& p, const Cell32& c, const Bin32& b, float cth, float sth,
                                           float a) {
     float g = 0.0f;
     if (p.has_wind) {

@@ -14,6 +14,7 @@
 //    ~2e9) and of the weight sum: four MUFU ops per face and element.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <type_traits>
 
 #include "rpl_device.cuh"
@@ -25,8 +26,6 @@ namespace rpl {
 namespace {
 
 constexpr unsigned FULL = 0xffffffffu;
-constexpr int TX = 8, TY = 4;             // tile of horizontal cells per CTA
-constexpr int RW = TX + 6, RH = TY + 6;   // staged rectangle (only its cross is loaded)
 constexpr int NB = 3;                     // plane buffers
 
 __device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
@@ -101,17 +100,22 @@ __device__ __forceinline__ float2 flux2(float2 m3, float2 m2, float2 m1, float2 
     return mul2(u, make_float2(px ? diff.x : -diff.x, py ? diff.y : -diff.y));
 }
 
-template <int L, bool REFRACT, bool SRC>
-__global__ void __launch_bounds__(TX* TY* L, 1) tile_kernel(const float* __restrict__ Nin, const float* N0, float* Nout,
-                                                          StageParams p) {
-    constexpr int KP = 2 * L;               // kappa slots per staged column
+// One CTA's work: stage update of the TX x TY tile `tile` (row-major over the tiles of the grid) for all
+// bins, with TX*TY*L threads. P is TileArgs seen through the kernel parameter bank (single-model kernel)
+// or a shared-memory copy (ensemble kernel).
+template <int L, int TX, int TY, bool REFRACT, bool SRC>
+__device__ __forceinline__ void tile_body(const TileArgs& p, int tile, float* smem) {
+    constexpr int RW = TX + 6, RH = TY + 6;   // staged rectangle (only its cross is loaded)
+    constexpr int KP = 2 * L;                 // kappa slots per staged column
     constexpr int THREADS = TX * TY * L;
-    constexpr int CROSS = RW * TY + 6 * TX;  // staged columns per plane
-    extern __shared__ __align__(16) float smem[];
-    const int Nx = (int)p.Nx, Ny = (int)p.Ny, Nk = (int)p.Nk, Np = (int)p.Np;
+    constexpr int CROSS = RW * TY + 6 * TX;   // staged columns per plane
+    const float* __restrict__ Nin = p.Nin;
+    const float* N0 = p.N0;
+    float* Nout = p.Nout;
+    const int Nx = p.Nx, Ny = p.Ny, Nk = p.Nk, Np = p.Np;
     const int64_t slice = (int64_t)Nx * Ny * Nk;
     const int tiles_x = (Nx + TX - 1) / TX;
-    const int i0 = (blockIdx.x % tiles_x) * TX, j0 = (blockIdx.x / tiles_x) * TY;
+    const int i0 = (tile % tiles_x) * TX, j0 = (tile / tiles_x) * TY;
     const int tid = threadIdx.x;
     const int l = tid % L;                    // lane within the cell
     const int cell = tid / L;                 // 0 .. TX*TY-1
@@ -127,7 +131,7 @@ __global__ void __launch_bounds__(TX* TY* L, 1) tile_kernel(const float* __restr
     // cp.async chunk descriptors (16-byte chunks of the cross columns), reused for every plane
     const int KC = Nk / 4;
     const int nchunks = CROSS * KC;
-    constexpr int MAXC = (CROSS * 8 + THREADS - 1) / THREADS;
+    constexpr int MAXC = (CROSS * (KP / 4) + THREADS - 1) / THREADS;
     int64_t goff[MAXC];
     int soff[MAXC];
 #pragma unroll
@@ -194,8 +198,8 @@ __global__ void __launch_bounds__(TX* TY* L, 1) tile_kernel(const float* __restr
         w0 = own[s2 * wr(-3)]; w1 = own[s2 * wr(-2)]; w2 = own[s2 * wr(-1)]; w3 = own[0];
         w4 = own[s2 * wr(1)]; w5 = own[s2 * wr(2)]; w6 = own[s2 * wr(3)];
     }
-    const float dx_inv = (float)p.dx_inv, dy_inv = (float)p.dy_inv, dk_inv = (float)p.dk_inv, dp_inv = (float)p.dp_inv;
-    const float dt = (float)p.dt, ca = (float)p.a, cb = (float)p.b;
+    const float dx_inv = p.dx_inv, dy_inv = p.dy_inv, dk_inv = p.dk_inv, dp_inv = p.dp_inv;
+    const float dt = p.dt, ca = p.a, cb = p.b;
     // kappa faces: face a between m0|m0+1 and face b between m0+1|m0+2
     const bool ha = (m0 - 2 >= 0) && (m0 + 3 <= Nk - 1);
     const bool hb = (m0 - 1 >= 0) && (m0 + 4 <= Nk - 1);
@@ -327,29 +331,112 @@ __global__ void __launch_bounds__(TX* TY* L, 1) tile_kernel(const float* __restr
     asm volatile("cp.async.wait_group 0;");
 }
 
+// Single-model kernel: 8 x 4 tiles, one CTA per tile.
 template <int L, bool REFRACT, bool SRC>
-cudaError_t launch_variant(const StageParams& p, const float* in, const float* n0, float* out, int tiles,
-                           cudaStream_t s) {
-    const size_t smem = (size_t)NB * RW * RH * 2 * L * sizeof(float);
+__global__ void __launch_bounds__(8 * 4 * L, 1) tile_kernel(const TileArgs p) {
+    extern __shared__ __align__(16) float smem[];
+    tile_body<L, 8, 4, REFRACT, SRC>(p, blockIdx.x, smem);
+}
+
+// Ensemble kernel: a persistent grid of ENSEMBLE_THREADS-thread CTAs takes work items (member, tile,
+// tile shape) from one atomic counter until the list is exhausted; no CTA ever waits for another.
+// The member's arguments are copied to shared memory per item.
+template <bool REFRACT>
+__global__ void __launch_bounds__(ENSEMBLE_THREADS, 1)
+    ensemble_kernel(const TileArgs* __restrict__ args, const int4* __restrict__ items, int nitems,
+                    unsigned int* counter) {
+    extern __shared__ __align__(16) float smem[];
+    __shared__ TileArgs s_args;
+    __shared__ int s_item;
+    constexpr int WORDS = (int)(sizeof(TileArgs) / 4);
+    static_assert(sizeof(TileArgs) % 4 == 0 && WORDS <= ENSEMBLE_THREADS, "TileArgs copy");
+    for (;;) {
+        if (threadIdx.x == 0) s_item = (int)atomicAdd(counter, 1u);
+        __syncthreads();
+        const int it = s_item;
+        if (it >= nitems) break;
+        const int4 w = __ldg(items + it);
+        if (threadIdx.x < WORDS)
+            reinterpret_cast<int*>(&s_args)[threadIdx.x] = __ldg(reinterpret_cast<const int*>(args + w.x) + threadIdx.x);
+        __syncthreads();
+        switch (w.z) {
+            case 0: tile_body<kEnsembleShapes[0].L, kEnsembleShapes[0].TX, kEnsembleShapes[0].TY, REFRACT, false>(s_args, w.y, smem); break;
+            case 1: tile_body<kEnsembleShapes[1].L, kEnsembleShapes[1].TX, kEnsembleShapes[1].TY, REFRACT, false>(s_args, w.y, smem); break;
+            case 2: tile_body<kEnsembleShapes[2].L, kEnsembleShapes[2].TX, kEnsembleShapes[2].TY, REFRACT, false>(s_args, w.y, smem); break;
+            case 3: tile_body<kEnsembleShapes[3].L, kEnsembleShapes[3].TX, kEnsembleShapes[3].TY, REFRACT, false>(s_args, w.y, smem); break;
+            case 4: tile_body<kEnsembleShapes[4].L, kEnsembleShapes[4].TX, kEnsembleShapes[4].TY, REFRACT, false>(s_args, w.y, smem); break;
+            case 5: tile_body<kEnsembleShapes[5].L, kEnsembleShapes[5].TX, kEnsembleShapes[5].TY, REFRACT, false>(s_args, w.y, smem); break;
+            case 6: tile_body<kEnsembleShapes[6].L, kEnsembleShapes[6].TX, kEnsembleShapes[6].TY, REFRACT, false>(s_args, w.y, smem); break;
+            case 7: tile_body<kEnsembleShapes[7].L, kEnsembleShapes[7].TX, kEnsembleShapes[7].TY, REFRACT, false>(s_args, w.y, smem); break;
+            default: tile_body<kEnsembleShapes[8].L, kEnsembleShapes[8].TX, kEnsembleShapes[8].TY, REFRACT, false>(s_args, w.y, smem); break;
+        }
+        __syncthreads();  // the staged planes, s_args and s_item are reused by the next item
+    }
+}
+
+template <int L, bool REFRACT, bool SRC>
+cudaError_t launch_variant(const TileArgs& a, int tiles, cudaStream_t s) {
+    const size_t smem = tile_smem_bytes(L, 8, 4);
     auto k = tile_kernel<L, REFRACT, SRC>;
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k<<<tiles, TX * TY * L, smem, s>>>(in, n0, out, p);
+    k<<<tiles, 8 * 4 * L, smem, s>>>(a);
     return cudaGetLastError();
 }
 
 template <int L>
-cudaError_t launch_L(const Handle& h, const StageParams& p, const float* in, const float* n0, float* out,
-                     cudaStream_t s) {
-    const int tiles = (int)(((h.desc.Nx + TX - 1) / TX) * ((h.desc.Ny + TY - 1) / TY));
+cudaError_t launch_L(const Handle& h, const StageParams& p, const TileArgs& a, cudaStream_t s) {
+    const int tiles = (int)(((h.desc.Nx + 7) / 8) * ((h.desc.Ny + 3) / 4));
     const bool refract = p.transport == RPL_TRANSPORT_REFRACTION;
     const bool src = p.has_wind || p.has_diss;
-    if (refract) return src ? launch_variant<L, true, true>(p, in, n0, out, tiles, s)
-                            : launch_variant<L, true, false>(p, in, n0, out, tiles, s);
-    return src ? launch_variant<L, false, true>(p, in, n0, out, tiles, s)
-               : launch_variant<L, false, false>(p, in, n0, out, tiles, s);
+    if (refract) return src ? launch_variant<L, true, true>(a, tiles, s) : launch_variant<L, true, false>(a, tiles, s);
+    return src ? launch_variant<L, false, true>(a, tiles, s) : launch_variant<L, false, false>(a, tiles, s);
 }
 
 }  // namespace
+
+size_t tile_smem_bytes(int L, int TX, int TY) { return (size_t)NB * (TX + 6) * (TY + 6) * 2 * L * sizeof(float); }
+
+size_t ensemble_smem_bytes() {
+    size_t m = 0;
+    for (const TileShape& t : kEnsembleShapes) m = std::max(m, tile_smem_bytes(t.L, t.TX, t.TY));
+    return m;
+}
+
+TileArgs make_tile_args(const Handle& h, const StageParams& p, const void* Nin, const void* N0, void* Nout) {
+    TileArgs a{};
+    a.Nin = (const float*)Nin;
+    a.N0 = (const float*)N0;
+    a.Nout = (float*)Nout;
+    a.coef = p.coef;
+    a.trig32 = p.trig32;
+    a.cg32 = p.cg32;
+    a.cs32 = p.cs32;
+    a.cell32 = p.cell32;
+    a.bin32 = p.bin32;
+    a.err = p.err;
+    a.Nx = (int)h.desc.Nx;
+    a.Ny = (int)h.desc.Ny;
+    a.Nk = (int)h.desc.Nk;
+    a.Np = (int)h.desc.Np;
+    a.stage = p.stage;
+    a.cg_per_cell = p.cg_per_cell;
+    a.has_wind = p.has_wind;
+    a.stress_cap = p.stress_cap;
+    a.has_diss = p.has_diss;
+    a.dx_inv = (float)p.dx_inv;
+    a.dy_inv = (float)p.dy_inv;
+    a.dk_inv = (float)p.dk_inv;
+    a.dp_inv = (float)p.dp_inv;
+    a.dt = (float)p.dt;
+    a.a = (float)p.a;
+    a.b = (float)p.b;
+    a.wind_K32 = p.wind_K32;
+    a.von_karman32 = p.von_karman32;
+    a.z_alpha32 = p.z_alpha32;
+    a.p_in = (float)p.p_in;
+    a.ds_p = (float)p.ds_p;
+    return a;
+}
 
 bool tile32_supported(const Handle& h) {
     const rpl_desc& d = h.desc;
@@ -357,15 +444,41 @@ bool tile32_supported(const Handle& h) {
            d.Nk <= 32 && (d.transport != RPL_TRANSPORT_REFRACTION || d.Np >= 3) && d.Nx >= 3 && d.Ny >= 3;
 }
 
+int tile_lanes(int64_t Nk) { return Nk <= 8 ? 4 : (Nk <= 16 ? 8 : 16); }
+
 cudaError_t launch_tile32(const Handle& h, const StageParams& p, const void* Nin, const void* N0, void* Nout,
                           cudaStream_t s) {
-    const int Nk = (int)h.desc.Nk;
-    const float* in = (const float*)Nin;
-    const float* n0 = (const float*)N0;
-    float* out = (float*)Nout;
-    if (Nk <= 8) return launch_L<4>(h, p, in, n0, out, s);
-    if (Nk <= 16) return launch_L<8>(h, p, in, n0, out, s);
-    return launch_L<16>(h, p, in, n0, out, s);
+    const TileArgs a = make_tile_args(h, p, Nin, N0, Nout);
+    switch (tile_lanes(h.desc.Nk)) {
+        case 4: return launch_L<4>(h, p, a, s);
+        case 8: return launch_L<8>(h, p, a, s);
+        default: return launch_L<16>(h, p, a, s);
+    }
+}
+
+cudaError_t prepare_ensemble_kernels() {
+    const int smem = (int)ensemble_smem_bytes();
+    cudaError_t e = cudaFuncSetAttribute(ensemble_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(ensemble_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    return e;
+}
+
+int ensemble_grid(bool refract, int device) {
+    int sms = 0, per_sm = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    const int smem = (int)ensemble_smem_bytes();
+    if (refract) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ensemble_kernel<true>, ENSEMBLE_THREADS, smem);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ensemble_kernel<false>, ENSEMBLE_THREADS, smem);
+    return std::max(1, sms) * std::max(1, per_sm);
+}
+
+cudaError_t launch_ensemble_stage(bool refract, const TileArgs* d_args, const int4* d_items, int nitems,
+                                  unsigned int* d_counter, int grid, cudaStream_t s) {
+    const size_t smem = ensemble_smem_bytes();
+    if (refract) ensemble_kernel<true><<<grid, ENSEMBLE_THREADS, smem, s>>>(d_args, d_items, nitems, d_counter);
+    else ensemble_kernel<false><<<grid, ENSEMBLE_THREADS, smem, s>>>(d_args, d_items, nitems, d_counter);
+    return cudaGetLastError();
 }
 
 }  // namespace rpl

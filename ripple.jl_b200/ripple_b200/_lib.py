@@ -55,6 +55,11 @@ class RplSources(ctypes.Structure):
     ]
 
 
+class RplEnsembleOptions(ctypes.Structure):
+    _fields_ = [("abi_version", _i32), ("use_graph", _i32), ("autotune", _i32), ("reserved", _i32),
+                ("autotune_cache", ctypes.c_char_p)]
+
+
 class RplError(RuntimeError):
     """A librpl.so call failed; .code is the rpl_status."""
 
@@ -90,6 +95,17 @@ _SIGNATURES = {
     "rpl_device_bytes": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(_i64)]),
     "rpl_diagnostics_static": (ctypes.c_int, [ctypes.c_void_p, _i32, _i64, _i64, _i64, _i64, ctypes.c_void_p,
                                               _d, _d] + [ctypes.c_void_p] * 6),
+    "rpl_ensemble_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), _dp, _i32,
+                                           ctypes.POINTER(RplEnsembleOptions), ctypes.POINTER(ctypes.c_void_p)]),
+    "rpl_ensemble_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "rpl_ensemble_step": (ctypes.c_int, [ctypes.c_void_p, _i64]),
+    "rpl_ensemble_step_async": (ctypes.c_int, [ctypes.c_void_p, _i64]),
+    "rpl_ensemble_step_sequential_async": (ctypes.c_int, [ctypes.c_void_p, _i64]),
+    "rpl_ensemble_sync": (ctypes.c_int, [ctypes.c_void_p]),
+    "rpl_ensemble_autotune": (ctypes.c_int, [ctypes.c_void_p, _i32]),
+    "rpl_ensemble_shape": (ctypes.c_int, [ctypes.c_void_p, _i32, ctypes.POINTER(_i32), ctypes.POINTER(_i32),
+                                          ctypes.POINTER(_i32)]),
+    "rpl_ensemble_set_stream": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "rpl_last_error": (ctypes.c_char_p, []),
     "rpl_abi_version": (ctypes.c_int, []),
 }

@@ -95,8 +95,9 @@ def jonswap_spectrum(kappa, phi, kp=0.03, gamma=3.3, s=10, phi0=math.pi / 4):
 
 
 def seamount_eddies(N=1024, Nz=32, Nk=32, Np=36, nsteps=200, seed=2, L=1024 * 5000.0, cfl=0.4,
-                    n0_dtype=np.float64):
-    """Reduced N keeps the 5120 km domain (coarser cells), so seamounts and eddies keep their extent."""
+                    n0_dtype=np.float64, peak_current=0.5, n_eddies=8):
+    """Reduced N keeps the 5120 km domain (coarser cells), so seamounts and eddies keep their extent.
+    peak_current / n_eddies change the eddy field (the ensemble members use them)."""
     dx = L / N
     grid = RectilinearGrid(size=(N, N, Nz), x=(0.0, L), y=(0.0, L), z=(-4000.0, 0.0),
                            topology=("Periodic", "Periodic", "Bounded"))
@@ -116,11 +117,11 @@ def seamount_eddies(N=1024, Nz=32, Nk=32, Np=36, nsteps=200, seed=2, L=1024 * 50
     depth = np.maximum(depth, 100.0)
     us = np.zeros((N, N))
     vs = np.zeros((N, N))
-    for _ in range(8):
+    for _ in range(n_eddies):
         R = rng.uniform(30e3, 120e3)
         cx, cy = rng.uniform(0, L), rng.uniform(0, L)
         sgn = 1.0 if rng.uniform() < 0.5 else -1.0
-        A = 0.5 * R * math.exp(0.5) / math.sqrt(2.0)   # peak azimuthal speed 0.5 m/s at r = R/sqrt(2)
+        A = peak_current * R * math.exp(0.5) / math.sqrt(2.0)   # peak azimuthal speed at r = R/sqrt(2)
         dX, dY = _periodic_delta(X, cx, L), _periodic_delta(Y, cy, L)
         e = np.exp(-(dX ** 2 + dY ** 2) / R ** 2)
         us += sgn * A * (2 * dY / R ** 2) * e
@@ -172,3 +173,30 @@ def hurricane_swell(N=768, Nk=32, Np=36, nsteps=1000, L=768 * 10000.0, cfl=0.4, 
     return Workload("hurricane_swell", grid, sg, depth, N0, dt, nsteps, sources=sources,
                     notes={"track": "start (Lx/2, 0.2 Ly), +y at 5 m/s", "radius": 500e3,
                            "inflow_angle_deg": 20.0, "dt_rule": f"CFL {cfl}"})
+
+
+ENSEMBLE_SIZES = (64, 128, 256, 384)
+ENSEMBLE_SPECTRA = ((16, 24), (24, 36), (32, 36))
+
+
+def ensemble_members(count=64, seed=4, nsteps=500, sizes=ENSEMBLE_SIZES, spectra=ENSEMBLE_SPECTRA, dx=5000.0,
+                     Nz=16, n0_dtype=np.float32):
+    """The batching-form ensemble: `count` independent members, each drawn with one seeded generator:
+    grid N x N x Nz (N uniform from `sizes`, dx = 5 km, periodic), spectral grid uniform from `spectra`
+    (32/24/16 log kappa 0.002-0.5 x 36/24 directions), depth 4000 m minus three seeded seamounts, and
+    either one vortex or 8 eddies (even odds) with peak current U0 uniform in [0.1, 0.8] m/s decaying as
+    exp(z/200 m); JONSWAP-like N0; dt from each member's own CFL. A generator yields the members one at a
+    time so the caller can build a model and drop the host arrays before the next one."""
+    rng = np.random.default_rng(seed)
+    for i in range(count):
+        N = int(sizes[int(rng.integers(len(sizes)))])
+        Nk, Np = spectra[int(rng.integers(len(spectra)))]
+        U0 = float(rng.uniform(0.1, 0.8))
+        vortex = bool(rng.uniform() < 0.5)
+        member_seed = int(rng.integers(2 ** 31))
+        w = seamount_eddies(N=N, Nz=Nz, Nk=Nk, Np=Np, nsteps=nsteps, seed=member_seed, L=N * dx,
+                            n0_dtype=n0_dtype, peak_current=U0, n_eddies=1 if vortex else 8)
+        w.name = f"ensemble_member_{i}"
+        w.notes.update({"member": i, "U0": U0, "currents": "vortex" if vortex else "8 eddies",
+                        "member_seed": member_seed})
+        yield w
