@@ -233,6 +233,68 @@ int rpl_ensemble_shape(const rpl_ensemble* e, int32_t member, int32_t* lanes, in
 /* Run on the caller's CUDA stream (cudaStream_t on the members' device); invalidates the graph. */
 int rpl_ensemble_set_stream(rpl_ensemble* e, void* stream);
 
+/* ---- Learned source (the learned form) ----
+ * No counterpart in the reference. A small MLP stands in for the per-cell source-term tendency of
+ * PrecomputedSources (precomputed_sources.jl:396-439: stress-capped wind input + whitecapping): inputs
+ * are the cell's Nk*Np-bin log action spectrum and 4 extras (U10 / 30, sin and cos of the wind
+ * direction, log10(depth) / 4), three GELU hidden layers, output y per bin with source rate S / N =
+ * target_scale * sinh(y); the stage then adds N * rate. BF16 weights and activations, FP32
+ * accumulation on the tensor cores (tcgen05), FP32 master weights trained with Adam by the library's
+ * own forward and backward kernels. Training data come from the plain FP32 sources
+ * (rpl_learned_sample). Cells whose inputs leave the training ranges fall back to the plain sources. */
+typedef struct rpl_mlp rpl_mlp;
+
+typedef struct rpl_mlp_desc {
+    int32_t abi_version;   /* RPL_ABI_VERSION */
+    int32_t nbins;         /* spectral inputs and outputs (Nk * Np), a multiple of 128 */
+    int32_t hidden;        /* width of the three hidden layers, a multiple of 256 */
+    int32_t rows;          /* rows of one pass (training batch capacity, inference chunk), multiple of 128 */
+    int32_t device;
+    int32_t reserved;
+    uint64_t seed;         /* weight initialisation */
+    float feature_shift;   /* input x = (log(max(N, log_floor)) - feature_shift) / feature_scale */
+    float feature_scale;
+    float log_floor;
+    float target_scale;    /* network output y = asinh(rate / target_scale) */
+} rpl_mlp_desc;
+
+int rpl_mlp_create(const rpl_mlp_desc* d, rpl_mlp** out);
+int rpl_mlp_destroy(rpl_mlp* m);
+/* Stream of the network's work (a cudaStream_t on its device; NULL: the legacy default stream). Until
+ * this is called the network uses a non-blocking stream of its own. The device arrays passed to
+ * rpl_mlp_train_step / _gradients / _forward are read and written in that stream's order, so a caller
+ * whose allocator recycles memory per stream (PyTorch's) passes its own stream. */
+int rpl_mlp_set_stream(rpl_mlp* m, void* stream);
+/* Parameters as one FP32 vector: W1 (hidden x nbins), W1e (hidden x 4), b1, W2 (hidden x hidden), b2, W3,
+ * b3, W4 (nbins x hidden), b4 (nbins); matrices row-major (output index slowest). */
+int rpl_mlp_param_count(const rpl_mlp* m, int64_t* count);
+int rpl_mlp_get_params(rpl_mlp* m, float* host);
+int rpl_mlp_set_params(rpl_mlp* m, const float* host);
+/* Training rows live on the device: X (n x nbins BF16 features), E (n x 4 FP32 extras), T (n x nbins FP32
+ * targets). `rows` (device int32, B of them, B a multiple of 128 and <= desc.rows, each < n) picks the
+ * batch. Loss = mean squared error over the batch's outputs. rpl_mlp_train_step applies one Adam step
+ * (lr, betas 0.9 / 0.999, eps 1e-8; loss may be NULL); rpl_mlp_gradients returns the gradient (host,
+ * parameter layout) and the loss without updating. */
+int rpl_mlp_train_step(rpl_mlp* m, const void* X, const float* E, const float* T, const int32_t* rows,
+                       int32_t B, float lr, double* loss);
+int rpl_mlp_gradients(rpl_mlp* m, const void* X, const float* E, const float* T, const int32_t* rows,
+                      int32_t B, float* grads, double* loss);
+/* Network output Y (n x nbins FP32, device) for n rows of device X, E; n a multiple of 128. */
+int rpl_mlp_forward(rpl_mlp* m, const void* X, const float* E, int64_t n, float* Y);
+/* The tensor-core GEMM alone (for testing): C (M x N FP32) = A (M x K BF16) * B (N x K BF16)^T, device
+ * row-major arrays, M % 128 == 0, N % 128 == 0, K % 64 == 0; stream NULL = default. */
+int rpl_gemm_bf16(const void* A, const void* B, float* C, int32_t M, int32_t N, int32_t K, void* stream);
+/* Training pairs of the FP32 handle's current state and clock from its plain sources: for every cell c
+ * (c = i + Nx j) row c of X, E and T (device arrays of Nx*Ny rows; T = asinh(rate / target_scale)). */
+int rpl_learned_sample(rpl_handle* h, const rpl_mlp* m, void* X, float* E, float* T);
+/* Use `m` (NULL: back to the plain sources) for the handle's sources. lo, hi: host arrays of nbins + 4
+ * input bounds; a cell with any input outside [lo, hi] uses the plain sources. */
+int rpl_set_learned_source(rpl_handle* h, rpl_mlp* m, const float* lo, const float* hi);
+/* Network outputs y of the most recent stage (host, Nx*Ny rows of nbins, row c = cell i + Nx j). */
+int rpl_learned_outputs(rpl_handle* h, float* Y);
+/* Cells that fell back to the plain sources in the most recent stage. */
+int rpl_learned_fallback_cells(rpl_handle* h, int64_t* count);
+
 /* Device bytes held by the handle. */
 int rpl_device_bytes(rpl_handle* h, int64_t* bytes);
 /* Thread-local message of the last failing call on this thread ("" if none). */

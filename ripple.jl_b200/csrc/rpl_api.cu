@@ -69,6 +69,7 @@ cudaError_t dalloc(Handle* h, T** p, size_t count) {
 }
 
 void free_all(Handle* h) {
+    rpl::free_learned(h);
     void* ptrs[] = {h->N, h->A, h->B, h->d_kappa, h->d_phi, h->d_cos, h->d_sin, h->d_weights, h->d_cgx,
                     h->d_cgy, h->d_cgmag, h->d_depth, h->d_coupling, h->d_wind, h->d_diag, h->d_err,
                     h->d_coef, h->d_tab32, h->d_cell32, h->d_bin32};
@@ -95,6 +96,7 @@ int check_error_word(Handle* h) {
         RPL_CUDA(cudaMemsetAsync(h->d_err, 0, sizeof(unsigned int), h->stream));
         RPL_CUDA(cudaStreamSynchronize(h->stream));
         if (w & 2u) return fail(RPL_ERR_NONFINITE, "non-finite values in the action passed in");
+        if (w & 4u) return fail(RPL_ERR_DEVICE, "a tensor-core GEMM of the learned source gave up waiting");
         return fail(RPL_ERR_DEVICE, "a stage kernel produced non-finite wave action (time step too large?)");
     }
     return RPL_OK;
@@ -109,7 +111,8 @@ int launch_step(Handle* h, double dt, int stage_only) {
         void* Nout = stage == 1 ? h->A : (stage == 2 ? h->B : h->N);
         if (sources) {
             if (stage == 1) RPL_CUDA(rpl::launch_wind(*h, h->time, s));
-            if (h->src.stress_cap) RPL_CUDA(rpl::launch_stress_factor(*h, Nin, s));
+            if (h->learned) RPL_CUDA(rpl::launch_learned_stage_prep(*h, Nin, s));
+            else if (h->src.stress_cap) RPL_CUDA(rpl::launch_stress_factor(*h, Nin, s));
         }
         const rpl::StageParams p = rpl::make_params(*h, dt, stage);
         RPL_CUDA(rpl::launch_stage(*h, p, Nin, h->N, Nout, s));

@@ -42,6 +42,10 @@ struct StageParams {
     const float* w32;                       // (Nk,Np): spectral cell measures, FP32
     const float* cell32;                    // (Nx*Ny) records of 8 floats: wind constants (rpl_src32.cuh)
     const float* bin32;                     // Nk records of 8 floats: per-kappa source constants
+    const float* lrate;                     // learned source: (cells x Nk*Np) network outputs, bin m + Nk n
+    const unsigned int* lflag;              // learned source: per cell, nonzero = use the plain sources
+    float lscale;                           // learned source: rate = lscale * sinh(network output)
+    int learned;                            // 1: sources from the learned network (with per-cell fallback)
     // sources
     int has_wind, stress_cap, has_diss;
     const double* wind_U10;                 // (Nx,Ny)
@@ -71,7 +75,10 @@ struct TileArgs {
     int Nx, Ny, Nk, Np, stage, cg_per_cell, has_wind, stress_cap, has_diss, pad0;
     float dx_inv, dy_inv, dk_inv, dp_inv, dt, a, b;
     float wind_K32, von_karman32, z_alpha32, p_in, ds_p;
-    float pad1, pad2;
+    float lscale;
+    const float* lrate;
+    const unsigned int* lflag;
+    int learned, pad1;
 };
 
 // Tile shapes (kappa-pair lanes per cell L, tile TX x TY) compiled into the ensemble kernel; every
@@ -114,6 +121,14 @@ struct Handle {
     float* d_tab32 = nullptr;      // FP32 copies: 4*Np trig, 2*Nk*Np group velocity, 2*Np cos/sin, Nk*Np weights
     float* d_cell32 = nullptr;     // (Nx*Ny) x 8 floats of per-cell wind constants
     float* d_bin32 = nullptr;      // Nk x 8 floats of per-kappa source constants
+    // learned source (rpl_learned.cu)
+    rpl_mlp* learned = nullptr;
+    void* d_lx = nullptr;          // (rows x nbins) BF16 features, rows = cells rounded up to 128
+    float* d_le = nullptr;         // (rows x 4) extras
+    float* d_lr = nullptr;         // (rows x nbins) network outputs
+    unsigned int* d_lflag = nullptr;  // per cell: inputs outside the bounds -> plain sources
+    float* d_lbounds = nullptr;    // lo[nbins + 4], hi[nbins + 4]
+    int64_t lrows = 0;
     bool currents_set = false;
     // sources
     rpl_sources src{};
@@ -131,6 +146,12 @@ struct Handle {
     int64_t bytes = 0;
 };
 
+// Learned-source network internals (rpl_mlp.cu, rpl_learned.cu).
+int mlp_nbins(const rpl_mlp* m);
+const rpl_mlp_desc& mlp_desc(const rpl_mlp* m);
+cudaError_t launch_learned_stage_prep(const Handle& h, const void* Nin, cudaStream_t s);
+void free_learned(Handle* h);
+
 // Sets the thread-local message rpl_last_error() returns (rpl_api.cu).
 void set_last_error(const std::string& msg);
 
@@ -141,7 +162,7 @@ cudaError_t launch_doppler(const Handle& h, int64_t Nz, const double* d_u, const
 cudaError_t launch_gradients(const Handle& h, cudaStream_t s);
 cudaError_t launch_cg_field(const Handle& h, cudaStream_t s);
 cudaError_t launch_wind(const Handle& h, double t, cudaStream_t s);
-cudaError_t launch_stress_factor(const Handle& h, const void* Nin, cudaStream_t s);
+cudaError_t launch_stress_factor(const Handle& h, const void* Nin, cudaStream_t s, const unsigned int* only = nullptr);
 cudaError_t launch_diagnostics(const Handle& h, const void* Nin, cudaStream_t s);
 cudaError_t launch_scan_nonfinite(const Handle& h, const void* buf, cudaStream_t s);
 

@@ -375,11 +375,12 @@ cudaError_t launch_wind(const Handle& h, double t, cudaStream_t s) {
 // its bins over the direction ring in FP32, then the warp reduces. Writes the factor to the FP32 cell
 // record (slot 5) and to the FP64 factor field.
 __global__ void stress32_kernel(const float* __restrict__ N, StageParams p, float rho_w_g, float rho_air,
-                                float* cell32, double* __restrict__ factor) {
+                                float* cell32, double* __restrict__ factor, const unsigned int* __restrict__ only) {
     const int64_t c = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     const int64_t P = p.Nx * p.Ny;
     if (c >= P) return;  // uniform per warp
+    if (only && only[c] == 0) return;  // learned source: only cells that fall back need the cap
     const float* r = cell32 + 8 * c;
     const Cell32 q{r[0], r[1], r[2], r[3], r[4], 1.0f, 0.0f, 0.0f};
     float f = 1.0f;
@@ -412,7 +413,7 @@ __global__ void stress32_kernel(const float* __restrict__ N, StageParams p, floa
     }
 }
 
-cudaError_t launch_stress_factor(const Handle& h, const void* Nin, cudaStream_t s) {
+cudaError_t launch_stress_factor(const Handle& h, const void* Nin, cudaStream_t s, const unsigned int* only) {
     const rpl_desc& d = h.desc;
     const int64_t P = d.Nx * d.Ny;
     StageParams p = make_params(h, 1.0, 1);
@@ -422,7 +423,7 @@ cudaError_t launch_stress_factor(const Handle& h, const void* Nin, cudaStream_t 
                                                                  h.d_wind + 3 * P);
     else
         stress32_kernel<<<blocks_for(P * 32, 256), 256, 0, s>>>((const float*)Nin, p, (float)rho_w_g,
-                                                                (float)h.src.rho_air, h.d_cell32, h.d_wind + 3 * P);
+                                                                (float)h.src.rho_air, h.d_cell32, h.d_wind + 3 * P, only);
     return cudaGetLastError();
 }
 

@@ -71,4 +71,24 @@ __device__ __forceinline__ float source32(const P& p, const Cell32& c, const Bin
     return g;
 }
 
+// Source rate of one cell-bin, g / a for the g of source32 (the learned source's training target):
+// the stress-capped wind growth rate minus the whitecapping rate at action a.
+template <class P>
+__device__ __forceinline__ float rate32(const P& p, const Cell32& c, const Bin32& b, float cth, float sth, float a) {
+    float r = 0.0f;
+    if (p.has_wind) {
+        float cos_tu;
+        const float w = wind_rate32(p, c, b, cth, sth, cos_tu);
+        r = p.stress_cap ? w * c.factor : w;
+    }
+    if (p.has_diss) {
+        float ov = fmaf(a, b.skB, -1.0f);
+        const bool valid = a > 0.0f && ov > 0.0f;
+        ov = fminf(fmaxf(ov, 0.0f), 1e6f);
+        const float op = (p.ds_p == 2.0) ? ov * ov : pow_pos32(ov, (float)p.ds_p);
+        r -= valid ? b.dsK * op : 0.0f;
+    }
+    return r;
+}
+
 }  // namespace rpl

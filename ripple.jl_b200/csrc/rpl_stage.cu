@@ -426,6 +426,10 @@ StageParams make_params(const Handle& h, double dt, int stage) {
     p.w32 = h.d_tab32 + 6 * d.Np + 2 * d.Nk * d.Np;
     p.cell32 = h.d_cell32;
     p.bin32 = h.d_bin32;
+    p.learned = h.learned != nullptr;
+    p.lrate = h.d_lr;
+    p.lflag = h.d_lflag;
+    p.lscale = h.learned ? mlp_desc(h.learned).target_scale : 0.0f;
     p.has_wind = h.has_sources && h.src.wind_kind != RPL_WIND_NONE;
     p.stress_cap = h.has_sources && h.src.stress_cap;
     p.has_diss = h.has_sources && h.src.has_dissipation;

@@ -103,7 +103,8 @@ __device__ __forceinline__ float2 flux2(float2 m3, float2 m2, float2 m1, float2 
 // One CTA's work: stage update of the TX x TY tile `tile` (row-major over the tiles of the grid) for all
 // bins, with TX*TY*L threads. P is TileArgs seen through the kernel parameter bank (single-model kernel)
 // or a shared-memory copy (ensemble kernel).
-template <int L, int TX, int TY, bool REFRACT, bool SRC>
+// SRC: 0 no sources, 1 the plain FP32 sources, 2 the learned source with per-cell plain fallback.
+template <int L, int TX, int TY, bool REFRACT, int SRC>
 __device__ __forceinline__ void tile_body(const TileArgs& p, int tile, float* smem) {
     constexpr int RW = TX + 6, RH = TY + 6;   // staged rectangle (only its cross is loaded)
     constexpr int KP = 2 * L;                 // kappa slots per staged column
@@ -212,10 +213,17 @@ __device__ __forceinline__ void tile_body(const TileArgs& p, int tile, float* sm
     // source constants of this cell and of the lane's two kappa bins
     Cell32 wc{};
     Bin32 wb0{}, wb1{};
-    if constexpr (SRC) {
-        wc = load_cell32(p.cell32 + 8 * ((int64_t)jc * Nx + ic));
+    bool plain_src = SRC == 1;
+    const float* lrow = nullptr;
+    if constexpr (SRC != 0) {
+        const int64_t cidx = (int64_t)jc * Nx + ic;
+        wc = load_cell32(p.cell32 + 8 * cidx);
         wb0 = load_bin32(p.bin32 + 8 * mc);
         wb1 = load_bin32(p.bin32 + 8 * (mc + 1));
+        if constexpr (SRC == 2) {
+            plain_src = __ldg(p.lflag + cidx) != 0u;
+            lrow = p.lrate + cidx * ((int64_t)Nk * Np) + mc;
+        }
     }
 
     for (int n = 0; n < Np; ++n) {
@@ -307,10 +315,15 @@ __device__ __forceinline__ void tile_body(const TileArgs& p, int tile, float* sm
                                          V(3 * RW, m0), uy), f2(dy_inv));
             G = mul2(f2(-1.f), add2(fx, fy));
         }
-        if constexpr (SRC) {
-            const float2 cs = __ldg(p.cs32 + n);
-            G.x += source32(p, wc, wb0, cs.x, cs.y, c.x);
-            G.y += source32(p, wc, wb1, cs.x, cs.y, c.y);
+        if constexpr (SRC != 0) {
+            if (plain_src) {
+                const float2 cs = __ldg(p.cs32 + n);
+                G.x += source32(p, wc, wb0, cs.x, cs.y, c.x);
+                G.y += source32(p, wc, wb1, cs.x, cs.y, c.y);
+            } else {  // learned: N * rate, rate = lscale * sinh(network output of bin (m, n))
+                const float2 y = __ldg(reinterpret_cast<const float2*>(lrow + (int64_t)n * Nk));
+                G = fma2(mul2(c, f2(p.lscale)), make_float2(sinhf(y.x), sinhf(y.y)), G);
+            }
         }
         // stage update
         float2 st = fma2(f2(dt), G, c);
@@ -332,7 +345,7 @@ __device__ __forceinline__ void tile_body(const TileArgs& p, int tile, float* sm
 }
 
 // Single-model kernel: 8 x 4 tiles, one CTA per tile.
-template <int L, bool REFRACT, bool SRC>
+template <int L, bool REFRACT, int SRC>
 __global__ void __launch_bounds__(8 * 4 * L, 1) tile_kernel(const TileArgs p) {
     extern __shared__ __align__(16) float smem[];
     tile_body<L, 8, 4, REFRACT, SRC>(p, blockIdx.x, smem);
@@ -360,21 +373,21 @@ __global__ void __launch_bounds__(ENSEMBLE_THREADS, 1)
             reinterpret_cast<int*>(&s_args)[threadIdx.x] = __ldg(reinterpret_cast<const int*>(args + w.x) + threadIdx.x);
         __syncthreads();
         switch (w.z) {
-            case 0: tile_body<kEnsembleShapes[0].L, kEnsembleShapes[0].TX, kEnsembleShapes[0].TY, REFRACT, false>(s_args, w.y, smem); break;
-            case 1: tile_body<kEnsembleShapes[1].L, kEnsembleShapes[1].TX, kEnsembleShapes[1].TY, REFRACT, false>(s_args, w.y, smem); break;
-            case 2: tile_body<kEnsembleShapes[2].L, kEnsembleShapes[2].TX, kEnsembleShapes[2].TY, REFRACT, false>(s_args, w.y, smem); break;
-            case 3: tile_body<kEnsembleShapes[3].L, kEnsembleShapes[3].TX, kEnsembleShapes[3].TY, REFRACT, false>(s_args, w.y, smem); break;
-            case 4: tile_body<kEnsembleShapes[4].L, kEnsembleShapes[4].TX, kEnsembleShapes[4].TY, REFRACT, false>(s_args, w.y, smem); break;
-            case 5: tile_body<kEnsembleShapes[5].L, kEnsembleShapes[5].TX, kEnsembleShapes[5].TY, REFRACT, false>(s_args, w.y, smem); break;
-            case 6: tile_body<kEnsembleShapes[6].L, kEnsembleShapes[6].TX, kEnsembleShapes[6].TY, REFRACT, false>(s_args, w.y, smem); break;
-            case 7: tile_body<kEnsembleShapes[7].L, kEnsembleShapes[7].TX, kEnsembleShapes[7].TY, REFRACT, false>(s_args, w.y, smem); break;
-            default: tile_body<kEnsembleShapes[8].L, kEnsembleShapes[8].TX, kEnsembleShapes[8].TY, REFRACT, false>(s_args, w.y, smem); break;
+            case 0: tile_body<kEnsembleShapes[0].L, kEnsembleShapes[0].TX, kEnsembleShapes[0].TY, REFRACT, 0>(s_args, w.y, smem); break;
+            case 1: tile_body<kEnsembleShapes[1].L, kEnsembleShapes[1].TX, kEnsembleShapes[1].TY, REFRACT, 0>(s_args, w.y, smem); break;
+            case 2: tile_body<kEnsembleShapes[2].L, kEnsembleShapes[2].TX, kEnsembleShapes[2].TY, REFRACT, 0>(s_args, w.y, smem); break;
+            case 3: tile_body<kEnsembleShapes[3].L, kEnsembleShapes[3].TX, kEnsembleShapes[3].TY, REFRACT, 0>(s_args, w.y, smem); break;
+            case 4: tile_body<kEnsembleShapes[4].L, kEnsembleShapes[4].TX, kEnsembleShapes[4].TY, REFRACT, 0>(s_args, w.y, smem); break;
+            case 5: tile_body<kEnsembleShapes[5].L, kEnsembleShapes[5].TX, kEnsembleShapes[5].TY, REFRACT, 0>(s_args, w.y, smem); break;
+            case 6: tile_body<kEnsembleShapes[6].L, kEnsembleShapes[6].TX, kEnsembleShapes[6].TY, REFRACT, 0>(s_args, w.y, smem); break;
+            case 7: tile_body<kEnsembleShapes[7].L, kEnsembleShapes[7].TX, kEnsembleShapes[7].TY, REFRACT, 0>(s_args, w.y, smem); break;
+            default: tile_body<kEnsembleShapes[8].L, kEnsembleShapes[8].TX, kEnsembleShapes[8].TY, REFRACT, 0>(s_args, w.y, smem); break;
         }
         __syncthreads();  // the staged planes, s_args and s_item are reused by the next item
     }
 }
 
-template <int L, bool REFRACT, bool SRC>
+template <int L, bool REFRACT, int SRC>
 cudaError_t launch_variant(const TileArgs& a, int tiles, cudaStream_t s) {
     const size_t smem = tile_smem_bytes(L, 8, 4);
     auto k = tile_kernel<L, REFRACT, SRC>;
@@ -387,9 +400,13 @@ template <int L>
 cudaError_t launch_L(const Handle& h, const StageParams& p, const TileArgs& a, cudaStream_t s) {
     const int tiles = (int)(((h.desc.Nx + 7) / 8) * ((h.desc.Ny + 3) / 4));
     const bool refract = p.transport == RPL_TRANSPORT_REFRACTION;
-    const bool src = p.has_wind || p.has_diss;
-    if (refract) return src ? launch_variant<L, true, true>(a, tiles, s) : launch_variant<L, true, false>(a, tiles, s);
-    return src ? launch_variant<L, false, true>(a, tiles, s) : launch_variant<L, false, false>(a, tiles, s);
+    const int src = p.learned ? 2 : ((p.has_wind || p.has_diss) ? 1 : 0);
+    if (refract) {
+        if (src == 2) return launch_variant<L, true, 2>(a, tiles, s);
+        return src ? launch_variant<L, true, 1>(a, tiles, s) : launch_variant<L, true, 0>(a, tiles, s);
+    }
+    if (src == 2) return launch_variant<L, false, 2>(a, tiles, s);
+    return src ? launch_variant<L, false, 1>(a, tiles, s) : launch_variant<L, false, 0>(a, tiles, s);
 }
 
 }  // namespace
@@ -435,6 +452,10 @@ TileArgs make_tile_args(const Handle& h, const StageParams& p, const void* Nin, 
     a.z_alpha32 = p.z_alpha32;
     a.p_in = (float)p.p_in;
     a.ds_p = (float)p.ds_p;
+    a.learned = p.learned;
+    a.lrate = p.lrate;
+    a.lflag = p.lflag;
+    a.lscale = p.lscale;
     return a;
 }
 

@@ -12,6 +12,7 @@ from .sources import (BulkWindDrag, Clockwise, Counterclockwise, HollandHurrican
 from .model import (Clock, ProductField, Simulation, SpectralWaveModel, WENO, WaveActionField,
                     compute_tendencies, interior, run_, set_, time_step)
 from .ensemble import Ensemble
+from . import learned
 from .diagnostics import (diagnostics, m0, mean_direction, mean_period, root_mean_square_wavenumber,
                           significant_wave_height, total_action)
 

@@ -60,6 +60,12 @@ class RplEnsembleOptions(ctypes.Structure):
                 ("autotune_cache", ctypes.c_char_p)]
 
 
+class RplMlpDesc(ctypes.Structure):
+    _fields_ = [("abi_version", _i32), ("nbins", _i32), ("hidden", _i32), ("rows", _i32), ("device", _i32),
+                ("reserved", _i32), ("seed", ctypes.c_uint64), ("feature_shift", ctypes.c_float),
+                ("feature_scale", ctypes.c_float), ("log_floor", ctypes.c_float), ("target_scale", ctypes.c_float)]
+
+
 class RplError(RuntimeError):
     """A librpl.so call failed; .code is the rpl_status."""
 
@@ -106,6 +112,24 @@ _SIGNATURES = {
     "rpl_ensemble_shape": (ctypes.c_int, [ctypes.c_void_p, _i32, ctypes.POINTER(_i32), ctypes.POINTER(_i32),
                                           ctypes.POINTER(_i32)]),
     "rpl_ensemble_set_stream": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "rpl_mlp_create": (ctypes.c_int, [ctypes.POINTER(RplMlpDesc), ctypes.POINTER(ctypes.c_void_p)]),
+    "rpl_mlp_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "rpl_mlp_set_stream": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "rpl_mlp_param_count": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(_i64)]),
+    "rpl_mlp_get_params": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "rpl_mlp_set_params": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "rpl_mlp_train_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                          ctypes.c_void_p, _i32, ctypes.c_float, _dp]),
+    "rpl_mlp_gradients": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                         ctypes.c_void_p, _i32, ctypes.c_void_p, _dp]),
+    "rpl_mlp_forward": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, _i64, ctypes.c_void_p]),
+    "rpl_gemm_bf16": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, _i32, _i32, _i32,
+                                     ctypes.c_void_p]),
+    "rpl_learned_sample": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                          ctypes.c_void_p]),
+    "rpl_set_learned_source": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "rpl_learned_outputs": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "rpl_learned_fallback_cells": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(_i64)]),
     "rpl_last_error": (ctypes.c_char_p, []),
     "rpl_abi_version": (ctypes.c_int, []),
 }

@@ -198,6 +198,7 @@ class SpectralWaveModel:
         self.velocities = velocities
         self.timestepper = "RK3"
         self.precision = precision
+        self.device = device
         self.clock = clock if clock is not None else Clock()
         self.boundary_conditions = boundary_conditions
         Nx, Ny = grid.Nx, grid.Ny
