@@ -42,7 +42,11 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
-    ap.add_argument("--workload", default="seamount", choices=["seamount", "hurricane", "ensemble"])
+    ap.add_argument("--workload", default="seamount", choices=["seamount", "hurricane", "ensemble", "learned"])
+    ap.add_argument("--train-steps", type=int, default=6000, help="Adam steps (--workload learned)")
+    ap.add_argument("--snapshots", type=int, default=40, help="training snapshots per storm run (--workload learned)")
+    ap.add_argument("--calm-fraction", type=float, default=0.05,
+                    help="share of cells without source activity kept as training rows (--workload learned)")
     ap.add_argument("--members", type=int, default=64, help="ensemble members (--workload ensemble)")
     ap.add_argument("--autotune-cache", default="", help="tile-shape cache file (--workload ensemble)")
     ap.add_argument("--member-sizes", default="64,128,256,384",
@@ -52,11 +56,12 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
     if args.size <= 0:
-        args.size = 1024 if args.workload == "seamount" else 768
+        args.size = 1024 if args.workload in ("seamount", "ensemble") else 768
     return args
 
 
-WORKLOAD_NAMES = {"seamount": "seamount_eddies", "hurricane": "hurricane_swell", "ensemble": "ensemble_members"}
+WORKLOAD_NAMES = {"seamount": "seamount_eddies", "hurricane": "hurricane_swell", "ensemble": "ensemble_members",
+                  "learned": "hurricane_swell (learned source)"}
 
 
 def make_workload(name, n, nsteps, n0_dtype=np.float64):
@@ -469,6 +474,144 @@ def run_ensemble(args, rank, world, local_rank):
         dist.destroy_process_group()
 
 
+def run_learned(args, rank, world, local_rank):
+    """The learned form on the translating-hurricane configuration (--size^2 x 32 kappa x 36 directions,
+    --steps RK3 steps): training rows from two plain FP32 runs (this storm and a second seeded storm:
+    Vmax 40 m/s, start (0.3 L, 0.3 L), 7 m/s), the library's own training, then the same run with the
+    learned source and with the plain FP32 sources from the same start, both device-timed; the learned
+    run's Hs, spectra and total action against the plain run's."""
+    import torch
+    import ripple_b200 as rp
+    from ripple_b200 import _lib, learned, workloads
+
+    torch.cuda.set_device(local_rank)
+    try:
+        smi_id = "GPU-" + str(torch.cuda.get_device_properties(local_rank).uuid)
+    except Exception:
+        smi_id = str(local_rank)
+    n, K = args.size, args.steps
+    nb, hd = 32 * 36, 512
+    net = learned.SourceNetwork(nbins=nb, hidden=hd, rows=16384, seed=5, device=local_rank)
+    # 1. training rows from the plain sources
+    t0 = time.perf_counter()
+    storms = [dict(), dict(vmax=40.0, start=(0.3, 0.3), translation=7.0)]
+    every = max(1, K // max(1, args.snapshots))
+    gen = torch.Generator(device="cuda").manual_seed(7)
+    Xs, Es, Ts = [], [], []
+    for st in storms:
+        w = workloads.hurricane_swell(N=n, nsteps=K, n0_dtype=np.float32, **st)
+        m = w.model("fp32", device=local_rank)
+        for k in range(0, K, every):
+            X, E, T = learned.sample(m, net)
+            peak = T.abs().amax(1)
+            act = peak > 0.5
+            calm = (~act) & (torch.rand(peak.shape, device=peak.device, generator=gen) < args.calm_fraction)
+            keep = (act | calm).nonzero().squeeze(1)
+            Xs.append(X[keep])
+            Es.append(E[keep])
+            Ts.append(T[keep])
+            del X, E, T, peak, act, calm, keep
+            rp.time_step(m, w.dt, min(every, K - k))
+        m.close()
+    X, E, T = torch.cat(Xs), torch.cat(Es), torch.cat(Ts)
+    del Xs, Es, Ts
+    torch.cuda.synchronize()
+    t_data = time.perf_counter() - t0
+    lo, hi = learned.input_bounds(X, E)
+    # 2. training (the library's forward/backward/Adam kernels)
+    t0 = time.perf_counter()
+    losses = learned.train(net, X, E, T, steps=args.train_steps, batch=16384, lr=1e-3,
+                           weights=learned.row_weights(T), log_every=max(1, args.train_steps // 4))
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    rows = int(X.shape[0])
+    del X, E, T
+    # 3. the evaluation run, plain FP32 and learned, from the same start
+    w = workloads.hurricane_swell(N=n, nsteps=K, n0_dtype=np.float32)
+    res = {}
+    for mode in ("plain", "learned"):
+        warm = w.model("fp32", device=local_rank)     # warm-up on a throwaway copy
+        if mode == "learned":
+            learned.use_learned_source(warm, net, lo, hi)
+        rp.time_step(warm, w.dt, args.warmup)
+        warm.close()
+        m = w.model("fp32", device=local_rank)
+        if mode == "learned":
+            learned.use_learned_source(m, net, lo, hi)
+        lib, h = m._lib, m.handle
+        stream = torch.cuda.Stream(device=local_rank)
+        _lib.check(lib.rpl_set_stream(h, _lib.ctypes.c_void_p(stream.cuda_stream)))
+        _lib.check(lib.rpl_set_clock(h, 0.0, 0))
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        with ClockSampler(smi_id) as clk:
+            with torch.cuda.stream(stream):
+                start.record(stream)
+                _lib.check(lib.rpl_step_async(h, w.dt, K))
+                end.record(stream)
+            stream.synchronize()
+            _lib.check(lib.rpl_sync(h))
+        m._sync_clock()
+        ms = start.elapsed_time(end)
+        state = torch.empty(w.units, dtype=torch.float32, device="cuda")
+        _lib.check(lib.rpl_get_action_device(h, _lib.ctypes.c_void_p(state.data_ptr()), _lib.RPL_F32, 0))
+        d = rp.diagnostics(m.action)
+        res[mode] = dict(ms=ms, clocks=clk.summary(), N=state, Hs=d["Hs"], total=d["total_action"],
+                         fallback=learned.fallback_cells(m) if mode == "learned" else 0)
+        m.close()
+    a, b = res["learned"], res["plain"]
+    dN = float(torch.linalg.vector_norm((a["N"] - b["N"]).double()) / torch.linalg.vector_norm(b["N"].double()))
+    Nk, Np = 32, 36
+    spec = lambda v: v.double().reshape(Np, Nk, n * n).sum(2)   # device layout: bins (m, n) of all cells
+    dS = float(torch.linalg.vector_norm(spec(a["N"]) - spec(b["N"])) / torch.linalg.vector_norm(spec(b["N"])))
+    mask = b["Hs"] > 0.01 * b["Hs"].max()
+    dH = float(np.linalg.norm(a["Hs"] - b["Hs"]) / np.linalg.norm(b["Hs"]))
+    dHmax = float(np.max(np.abs(a["Hs"] - b["Hs"])[mask] / b["Hs"][mask]))
+    # 4. the network's forward GEMMs alone on one stage's rows, against the BF16 tensor-core peak
+    P = n * n
+    prow = (P + 127) // 128 * 128
+    Xf = torch.zeros((prow, nb), dtype=torch.bfloat16, device="cuda")
+    Ef = torch.zeros((prow, 4), device="cuda")
+    net.forward(Xf, Ef)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(3):
+        net.forward(Xf, Ef)
+    e1.record()
+    torch.cuda.synchronize()
+    fwd_ms = e0.elapsed_time(e1) / 3
+    flops = 2.0 * prow * (nb * hd + 2 * hd * hd + hd * nb)
+    try:
+        bf16_peak = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["bf16_tflops"])
+        peak_kind = "measured"
+    except Exception:
+        bf16_peak, peak_kind = 1590.0, "fallback"
+    peak, hbm_kind = peaks()
+    value = w.units * K / (a["ms"] / 1e3)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": K, "warmup": args.warmup,
+            "ms_per_step": a["ms"] / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 state, bf16 network", "impl": "learned",
+            "data": "synthetic (Holland hurricane on a linear track, uniform N0 = 1e-6)",
+            "config": {"workload": "hurricane_swell with the learned source", "grid": [n, n], "spectral": [Nk, Np],
+                       "network": f"{nb}+4 -> 3 x {hd} GELU -> {nb}, bf16 weights, fp32 accumulate",
+                       "plain_fp32_ms_per_step": b["ms"] / K, "speedup_vs_plain_fp32": b["ms"] / a["ms"],
+                       "Hs_relL2_vs_plain": dH, "Hs_max_rel_err_vs_plain": dHmax, "N_relL2_vs_plain": dN,
+                       "mean_spectrum_relL2_vs_plain": dS,
+                       "total_action_rel_diff": abs(a["total"] - b["total"]) / b["total"],
+                       "fallback_cells_last_stage": a["fallback"], "cells": P,
+                       "training_rows": rows, "training_steps": args.train_steps, "training_s": t_train,
+                       "data_generation_s": t_data, "losses": losses,
+                       "mlp_forward_ms_per_stage": fwd_ms, "mlp_forward_tflops": flops / fwd_ms / 1e9,
+                       "mlp_tensor_frac": flops / fwd_ms / 1e9 / bf16_peak, "bf16_peak_tflops": bf16_peak,
+                       "bf16_peak_kind": peak_kind},
+            "clocks": a["clocks"], "gpu_launches": None,
+        }
+        print(json.dumps(line), flush=True)
+    net.close()
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -479,6 +622,9 @@ def main():
         return
     if args.workload == "ensemble":
         run_ensemble(args, rank, world, local_rank)
+        return
+    if args.workload == "learned":
+        run_learned(args, rank, world, local_rank)
         return
     run_ours(args, rank, world, local_rank)
 

@@ -198,7 +198,8 @@ namespace rpl {
 int mlp_nbins(const rpl_mlp* m) { return m->nb; }
 const rpl_mlp_desc& mlp_desc(const rpl_mlp* m) { return m->d; }
 
-static int pick_bn(int M, int N) { return ((M / 128) * (N / 256) >= 148) ? 256 : 128; }
+// 256-column tiles when N allows them and they still give every SM a tile; else 128.
+static int pick_bn(int M, int N) { return (N % 256 == 0 && (M / 128) * (N / 256) >= 148) ? 256 : 128; }
 
 static cudaError_t gemm(rpl_mlp* m, GemmArgs g, cudaStream_t s) {
     g.err = m->d_err;

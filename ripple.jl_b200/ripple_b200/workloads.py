@@ -149,8 +149,10 @@ def seamount_eddies(N=1024, Nz=32, Nk=32, Np=36, nsteps=200, seed=2, L=1024 * 50
                            "N0": "JONSWAP kp=0.03 gamma=3.3, cos^20((phi-pi/4)/2), x-y envelope 1+0.3 sin cos"})
 
 
-def hurricane_swell(N=768, Nk=32, Np=36, nsteps=1000, L=768 * 10000.0, cfl=0.4, translation=5.0, Nz=24):
-    """Reduced N keeps the 7680 km domain (coarser cells)."""
+def hurricane_swell(N=768, Nk=32, Np=36, nsteps=1000, L=768 * 10000.0, cfl=0.4, translation=5.0, Nz=24,
+                    vmax=50.0, start=(0.5, 0.2), n0_dtype=np.float64):
+    """Reduced N keeps the 7680 km domain (coarser cells). vmax, start (fractions of the domain) and
+    translation (m/s along +y) vary the storm (the learned source's training runs use other storms)."""
     dx = L / N
     grid = RectilinearGrid(size=(N, N, Nz), x=(0.0, L), y=(0.0, L), z=(-4000.0, 0.0),
                            topology=("Periodic", "Periodic", "Bounded"))
@@ -162,14 +164,14 @@ def hurricane_swell(N=768, Nk=32, Np=36, nsteps=1000, L=768 * 10000.0, cfl=0.4, 
     cg0 = 0.5 * (1 + 2 * mu / math.sinh(2 * mu)) * math.sqrt(G * math.tanh(mu) / kappa[0])
     dt = cfl / (2 * cg0 / dx)
     T = nsteps * dt
-    start = (0.5 * L, 0.2 * L)
+    start = (start[0] * L, start[1] * L)
     track = LinearStormTrack([0.0, T], [start, (start[0], start[1] + translation * T)])
-    hurricane = HollandHurricaneWind(center=track, vmax=50.0, rmax=30e3, radius=500e3, shape_parameter=1.5,
+    hurricane = HollandHurricaneWind(center=track, vmax=vmax, rmax=30e3, radius=500e3, shape_parameter=1.5,
                                      inflow_angle=math.radians(20.0))
     sources = PrecomputedSources(
         wind_input=PressureCorrelationInput(drag=BulkWindDrag("linear"), wind=hurricane, direction=0.0),
         dissipation=LocalSaturationDissipation(B_r=1.05e-2, σ_power=1.0))
-    N0 = np.full((N, N, Nk, Np), 1e-6, order="F")
+    N0 = np.full((N, N, Nk, Np), 1e-6, dtype=n0_dtype, order="F")
     return Workload("hurricane_swell", grid, sg, depth, N0, dt, nsteps, sources=sources,
                     notes={"track": "start (Lx/2, 0.2 Ly), +y at 5 m/s", "radius": 500e3,
                            "inflow_angle_deg": 20.0, "dt_rule": f"CFL {cfl}"})
