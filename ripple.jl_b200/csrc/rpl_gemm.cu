@@ -2,13 +2,23 @@
 // tensor memory) with the fused epilogues the learned-source MLP needs.
 //
 // C[M x N] = A[M x K] * B[N x K]^T, A and B row-major with K contiguous ("K-major" operands).
-// One CTA of 128 threads owns a 128 x BN output tile. K advances in blocks of 64: every thread copies
-// its share of the A and B blocks into shared memory with cp.async, 128-byte swizzled so the tensor core
-// reads them through K-major descriptors; STAGES blocks are in flight. Thread 0 issues the four
-// K = 16 MMAs of a block into the TMEM accumulator and commits them to the block's mbarrier; a stage is
-// refilled only after that mbarrier reports the MMAs which read it complete. Every wait is bounded: on
-// timeout the kernel sets bit 4 of the error word, drains its copies, frees its TMEM and returns.
-// Requirements (checked by the host): M % 128 == 0, N % BN == 0, K % 64 == 0, 16-byte aligned rows.
+// A persistent, warp-specialised kernel: one CTA per SM walks the 128 x BN output tiles (tile t and
+// t + gridDim.x, ...). Its warps split the work:
+//   warps 0-3 (producers): copy 64-wide K blocks of A and B into a STAGES-deep ring of shared-memory
+//     stages with cp.async, 128-byte swizzled so the tensor core reads them through K-major descriptors;
+//     each thread's cp.async.mbarrier.arrive.noinc arrives on the stage's `full` barrier once its copies
+//     have landed, so the producers run up to STAGES blocks ahead without waiting for their own copies;
+//   warp 4 (MMA): waits `full`, fences the stage for the async proxy, issues the block's four K = 16
+//     tcgen05.mma into one of two TMEM
+//     accumulators (double buffered across tiles), commits the stage's `empty` barrier (the producers
+//     refill it) and, after a tile's last block, the accumulator's `acc_full` barrier;
+//   warps 5-12 (epilogue, two per TMEM lane quadrant, each taking half the columns): wait `acc_full`,
+//     read their lanes with tcgen05.ld, apply the fused epilogue, store, and arrive on `acc_empty` so the
+//     MMA warp may reuse that accumulator -- the epilogue of one tile overlaps the MMAs of the next.
+// Every wait is bounded and checks a shared abort flag: a wait that gives up sets bit 4 of the error word
+// and the flag, every role then leaves its loop, the copies in flight drain, TMEM is freed, and the
+// kernel returns. Requirements (checked by the host): M % 128 == 0, N % BN == 0, K % 64 == 0, 16-byte
+// aligned rows.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -19,10 +29,14 @@ namespace rpl {
 
 namespace {
 
-constexpr int BM = 128, BK = 64, THREADS = 128;
+constexpr int BM = 128, BK = 64, STAGES = 4;
+constexpr int PRODUCERS = 128;                 // warps 0-3
+constexpr int MMA_WARP = 4;
+constexpr int EPILOGUE = 256;                  // warps 5-12
+constexpr int THREADS = 13 * 32;               // producers + MMA warp + epilogue warps
 constexpr uint32_t WAIT_LIMIT = 1u << 24;
 
-template <int BN, int STAGES>
+template <int BN>
 struct GemmSmem {
     static constexpr int A_BYTES = BM * BK * 2;
     static constexpr int B_BYTES = BN * BK * 2;
@@ -37,162 +51,210 @@ __device__ __forceinline__ float gelu_grad(float z) {
     return cdf + z * pdf;
 }
 
-template <int BN, int STAGES, int EPI>
+// Arrives on `bar` when every cp.async this thread issued so far has completed (the arrival counts
+// toward the barrier's expected count).
+__device__ __forceinline__ void cp_async_arrive(uint32_t bar) {
+    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+// Bounded wait that also gives up once another role has aborted.
+__device__ __forceinline__ bool wait_phase(uint32_t bar, uint32_t parity, volatile int* abort_flag) {
+    for (uint32_t i = 0; i < WAIT_LIMIT; ++i) {
+        if (umma::mbar_try_wait(bar, parity)) return true;
+        if (*abort_flag) return false;
+    }
+    *abort_flag = 1;
+    return false;
+}
+
+// Fused epilogue of COLS accumulator columns for the thread holding row `row`: reads its TMEM lane
+// starting at TMEM address `trow`, writes output columns n0 .. n0 + COLS - 1.
+template <int COLS, int EPI>
+__device__ __forceinline__ void epilogue_cols(const GemmArgs& g, uint32_t trow, int row, int n0) {
+    float ex[4] = {0.f, 0.f, 0.f, 0.f};
+    if (EPI == EPI_BIAS_GELU && g.extra) {
+#pragma unroll
+        for (int e = 0; e < 4; ++e) ex[e] = g.extra[(int64_t)row * 4 + e];
+    }
+    for (int c0 = 0; c0 < COLS; c0 += 16) {
+        float v[16];
+        umma::tmem_ld16(trow + c0, v);
+        const int col = n0 + c0;
+        if (EPI == EPI_F32) {
+            float4* o = reinterpret_cast<float4*>(g.out_f32 + (int64_t)row * g.ldo + col);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) o[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+        } else if (EPI == EPI_BIAS) {
+            float4* o = reinterpret_cast<float4*>(g.out_f32 + (int64_t)row * g.ldo + col);
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+                o[i] = make_float4(v[4 * i] + g.bias[col + 4 * i], v[4 * i + 1] + g.bias[col + 4 * i + 1],
+                                   v[4 * i + 2] + g.bias[col + 4 * i + 2], v[4 * i + 3] + g.bias[col + 4 * i + 3]);
+        } else {
+            __nv_bfloat16 h[16];
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                float z = v[i];
+                if (EPI == EPI_BIAS_GELU) {
+                    z += g.bias[col + i];
+                    if (g.wextra) {
+                        const float* we = g.wextra + (int64_t)(col + i) * 4;
+                        z = fmaf(ex[0], we[0], fmaf(ex[1], we[1], fmaf(ex[2], we[2], fmaf(ex[3], we[3], z))));
+                    }
+                    if (g.out_f32) g.out_f32[(int64_t)row * g.ldo + col + i] = z;
+                    z = gelu(z);
+                } else {  // EPI_GELU_BWD: upstream gradient times GELU'(pre-activation)
+                    z *= gelu_grad(g.pre[(int64_t)row * g.ldp + col + i]);
+                }
+                h[i] = __float2bfloat16_rn(z);
+            }
+            if (g.out_bf16) {
+                uint4* o = reinterpret_cast<uint4*>(g.out_bf16 + (int64_t)row * g.ldh + col);
+                o[0] = *reinterpret_cast<const uint4*>(&h[0]);
+                o[1] = *reinterpret_cast<const uint4*>(&h[8]);
+            }
+            if (g.out_bf16_t) {
+#pragma unroll
+                for (int i = 0; i < 16; ++i) g.out_bf16_t[(int64_t)(col + i) * g.ldt + row] = h[i];
+            }
+        }
+    }
+}
+
+template <int BN, int EPI>
 __global__ void __launch_bounds__(THREADS, 1) gemm_kernel(const GemmArgs g) {
-    using S = GemmSmem<BN, STAGES>;
+    using S = GemmSmem<BN>;
     extern __shared__ uint8_t smem_raw[];
-    __shared__ uint64_t bars[STAGES];
+    __shared__ uint64_t full_bar[STAGES], empty_bar[STAGES], acc_full[2], acc_empty[2];
     __shared__ uint32_t s_tmem;
-    __shared__ int s_bad;
+    __shared__ int s_abort;
+    volatile int* abort_flag = &s_abort;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+    const int tiles_n = g.N / BN, tiles = (g.M / BM) * tiles_n;
     const int KB = g.K / BK;
     const uint32_t base = (umma::smem_u32(smem_raw) + 1023u) & ~1023u;
 
     if (tid == 0) {
-        for (int s = 0; s < STAGES; ++s) umma::mbar_init(umma::smem_u32(&bars[s]), 1);
+        for (int s = 0; s < STAGES; ++s) {
+            umma::mbar_init(umma::smem_u32(&full_bar[s]), PRODUCERS);
+            umma::mbar_init(umma::smem_u32(&empty_bar[s]), 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            umma::mbar_init(umma::smem_u32(&acc_full[b]), 1);
+            umma::mbar_init(umma::smem_u32(&acc_empty[b]), EPILOGUE);
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        s_bad = 0;
+        s_abort = 0;
     }
-    if (warp == 0) umma::tmem_alloc(umma::smem_u32(&s_tmem), BN);
+    if (warp == MMA_WARP) umma::tmem_alloc(umma::smem_u32(&s_tmem), 2 * BN);
     umma::fence_before_sync();
     __syncthreads();
     umma::fence_after_sync();
     const uint32_t tmem = s_tmem;
 
-    auto load = [&](int s, int kb) {
-        const uint32_t sa = base + s * S::STAGE, sb = sa + S::A_BYTES;
-        const int k0 = kb * BK;
+    if (warp < 4) {
+        // ---- producers ----
+        int64_t gcount = 0;  // K blocks issued by this CTA so far
+        for (int t = blockIdx.x; t < tiles && !*abort_flag; t += gridDim.x) {
+            const int m0 = (t / tiles_n) * BM, n0 = (t % tiles_n) * BN;
+            for (int kb = 0; kb < KB; ++kb, ++gcount) {
+                const int s = (int)(gcount % STAGES);
+                const int64_t use = gcount / STAGES;
+                if (use > 0 && !wait_phase(umma::smem_u32(&empty_bar[s]), (uint32_t)((use - 1) & 1), abort_flag)) break;
+                const uint32_t sa = base + s * S::STAGE, sb = sa + S::A_BYTES;
+                const int k0 = kb * BK;
 #pragma unroll 4
-        for (int q = tid; q < BM * 8; q += THREADS) {
-            const int r = q >> 3, c = q & 7;
-            umma::cp_async16(sa + r * 128 + ((c ^ (r & 7)) << 4), g.A + (int64_t)(m0 + r) * g.lda + k0 + c * 8);
-        }
+                for (int q = tid; q < BM * 8; q += PRODUCERS) {
+                    const int r = q >> 3, c = q & 7;
+                    umma::cp_async16(sa + r * 128 + ((c ^ (r & 7)) << 4), g.A + (int64_t)(m0 + r) * g.lda + k0 + c * 8);
+                }
 #pragma unroll 4
-        for (int q = tid; q < BN * 8; q += THREADS) {
-            const int r = q >> 3, c = q & 7;
-            umma::cp_async16(sb + r * 128 + ((c ^ (r & 7)) << 4), g.B + (int64_t)(n0 + r) * g.ldb + k0 + c * 8);
-        }
-    };
-
-    for (int s = 0; s < STAGES - 1; ++s) {
-        if (s < KB) load(s, s);
-        umma::cp_async_commit();
-    }
-    constexpr uint32_t IDESC = umma::idesc_bf16_f32(BM, BN);
-    for (int kb = 0; kb < KB; ++kb) {
-        const int s = kb % STAGES;
-        umma::cp_async_wait<STAGES - 2>();
-        umma::fence_proxy_async();
-        __syncthreads();
-        if (tid == 0) {
-            umma::fence_after_sync();
-            const uint32_t sa = base + s * S::STAGE, sb = sa + S::A_BYTES;
-#pragma unroll
-            for (int k = 0; k < BK / 16; ++k)
-                umma::mma_bf16(tmem, umma::kmajor_sw128_desc(sa + 32 * k), umma::kmajor_sw128_desc(sb + 32 * k), IDESC,
-                               (kb > 0 || k > 0) ? 1u : 0u);
-            umma::mma_commit(umma::smem_u32(&bars[s]));
-            // the stage refilled below was read by the MMAs of block kb - 1
-            if (kb >= 1 && kb + STAGES - 1 < KB) {
-                const int j = kb - 1;
-                if (!umma::mbar_wait_bounded(umma::smem_u32(&bars[j % STAGES]), (uint32_t)((j / STAGES) & 1),
-                                             WAIT_LIMIT))
-                    s_bad = 1;
+                for (int q = tid; q < BN * 8; q += PRODUCERS) {
+                    const int r = q >> 3, c = q & 7;
+                    umma::cp_async16(sb + r * 128 + ((c ^ (r & 7)) << 4), g.B + (int64_t)(n0 + r) * g.ldb + k0 + c * 8);
+                }
+                cp_async_arrive(umma::smem_u32(&full_bar[s]));
             }
         }
-        __syncthreads();
-        if (s_bad) break;
-        if (kb + STAGES - 1 < KB) load((kb + STAGES - 1) % STAGES, kb + STAGES - 1);
-        umma::cp_async_commit();
-    }
-    if (tid == 0 && !s_bad && KB > 0) {
-        const int j = KB - 1;
-        if (!umma::mbar_wait_bounded(umma::smem_u32(&bars[j % STAGES]), (uint32_t)((j / STAGES) & 1), WAIT_LIMIT))
-            s_bad = 1;
-    }
-    umma::cp_async_wait<0>();
-    __syncthreads();
-    umma::fence_after_sync();
-    const bool bad = s_bad != 0;
-    if (bad) {
-        if (tid == 0 && g.err) atomicOr(g.err, 4u);
-    } else {
-        // epilogue: warp w holds rows 32w .. 32w+31 of the tile in TMEM lanes 32w .. 32w+31
-        const int row = m0 + warp * 32 + lane;
-        const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
-        float ex[4] = {0.f, 0.f, 0.f, 0.f};
-        if (EPI == EPI_BIAS_GELU && g.extra) {
-#pragma unroll
-            for (int e = 0; e < 4; ++e) ex[e] = g.extra[(int64_t)row * 4 + e];
-        }
-        for (int c0 = 0; c0 < BN; c0 += 16) {
-            float v[16];
-            umma::tmem_ld16(trow + c0, v);
-            const int col = n0 + c0;
-            if (EPI == EPI_F32) {
-                float4* o = reinterpret_cast<float4*>(g.out_f32 + (int64_t)row * g.ldo + col);
-#pragma unroll
-                for (int i = 0; i < 4; ++i) o[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
-            } else if (EPI == EPI_BIAS) {
-                float4* o = reinterpret_cast<float4*>(g.out_f32 + (int64_t)row * g.ldo + col);
-#pragma unroll
-                for (int i = 0; i < 4; ++i)
-                    o[i] = make_float4(v[4 * i] + g.bias[col + 4 * i], v[4 * i + 1] + g.bias[col + 4 * i + 1],
-                                       v[4 * i + 2] + g.bias[col + 4 * i + 2], v[4 * i + 3] + g.bias[col + 4 * i + 3]);
-            } else {
-                __nv_bfloat16 h[16];
-#pragma unroll
-                for (int i = 0; i < 16; ++i) {
-                    float z = v[i];
-                    if (EPI == EPI_BIAS_GELU) {
-                        z += g.bias[col + i];
-                        if (g.wextra) {
-                            const float* we = g.wextra + (int64_t)(col + i) * 4;
-                            z = fmaf(ex[0], we[0], fmaf(ex[1], we[1], fmaf(ex[2], we[2], fmaf(ex[3], we[3], z))));
-                        }
-                        if (g.out_f32) g.out_f32[(int64_t)row * g.ldo + col + i] = z;
-                        z = gelu(z);
-                    } else {  // EPI_GELU_BWD: upstream gradient times GELU'(pre-activation)
-                        z *= gelu_grad(g.pre[(int64_t)row * g.ldp + col + i]);
+        asm volatile("cp.async.wait_all;" ::: "memory");
+    } else if (warp == MMA_WARP) {
+        // ---- MMA issue (one thread) ----
+        if (lane == 0) {
+            constexpr uint32_t IDESC = umma::idesc_bf16_f32(BM, BN);
+            int64_t gcount = 0;
+            int local = 0;
+            for (int t = blockIdx.x; t < tiles && !*abort_flag; t += gridDim.x, ++local) {
+                const int b = local & 1, ub = local >> 1;
+                if (ub > 0 && !wait_phase(umma::smem_u32(&acc_empty[b]), (uint32_t)((ub - 1) & 1), abort_flag)) break;
+                umma::fence_after_sync();
+                const uint32_t acc = tmem + (uint32_t)(b * BN);
+                bool ok = true;
+                for (int kb = 0; kb < KB; ++kb, ++gcount) {
+                    const int s = (int)(gcount % STAGES);
+                    if (!wait_phase(umma::smem_u32(&full_bar[s]), (uint32_t)((gcount / STAGES) & 1), abort_flag)) {
+                        ok = false;
+                        break;
                     }
-                    h[i] = __float2bfloat16_rn(z);
-                }
-                if (g.out_bf16) {
-                    uint4* o = reinterpret_cast<uint4*>(g.out_bf16 + (int64_t)row * g.ldh + col);
-                    o[0] = *reinterpret_cast<const uint4*>(&h[0]);
-                    o[1] = *reinterpret_cast<const uint4*>(&h[8]);
-                }
-                if (g.out_bf16_t) {
+                    umma::fence_proxy_async();  // the producers' cp.async writes, for the tensor core's reads
+                    umma::fence_after_sync();
+                    const uint32_t sa = base + s * S::STAGE, sb = sa + S::A_BYTES;
 #pragma unroll
-                    for (int i = 0; i < 16; ++i) g.out_bf16_t[(int64_t)(col + i) * g.ldt + row] = h[i];
+                    for (int k = 0; k < BK / 16; ++k)
+                        umma::mma_bf16(acc, umma::kmajor_sw128_desc(sa + 32 * k), umma::kmajor_sw128_desc(sb + 32 * k),
+                                       IDESC, (kb > 0 || k > 0) ? 1u : 0u);
+                    umma::mma_commit(umma::smem_u32(&empty_bar[s]));
                 }
+                if (!ok) break;
+                umma::mma_commit(umma::smem_u32(&acc_full[b]));
             }
         }
+        __syncwarp();
+    } else {
+        // ---- epilogue (warps 5-12: TMEM lane quadrant warp % 4, column half (warp - 5) / 4) ----
+        const int quad = warp & 3, half = (warp - 5) >> 2;
+        int local = 0;
+        for (int t = blockIdx.x; t < tiles && !*abort_flag; t += gridDim.x, ++local) {
+            const int b = local & 1;
+            if (!wait_phase(umma::smem_u32(&acc_full[b]), (uint32_t)((local >> 1) & 1), abort_flag)) break;
+            umma::fence_after_sync();
+            const int m0 = (t / tiles_n) * BM, n0 = (t % tiles_n) * BN;
+            const uint32_t trow = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(b * BN + half * (BN / 2));
+            epilogue_cols<BN / 2, EPI>(g, trow, m0 + quad * 32 + lane, n0 + half * (BN / 2));
+            umma::fence_before_sync();
+            mbar_arrive(umma::smem_u32(&acc_empty[b]));
+        }
     }
+    if (tid == 0 && *abort_flag && g.err) atomicOr(g.err, 4u);
     umma::fence_before_sync();
     __syncthreads();
-    if (warp == 0) {
+    if (warp == MMA_WARP) {
         umma::fence_after_sync();
-        umma::tmem_dealloc(tmem, BN);
+        umma::tmem_dealloc(tmem, 2 * BN);
     }
 }
 
-template <int BN, int STAGES, int EPI>
+template <int BN, int EPI>
 cudaError_t launch_bn(const GemmArgs& g, cudaStream_t s) {
-    using S = GemmSmem<BN, STAGES>;
-    auto k = gemm_kernel<BN, STAGES, EPI>;
+    using S = GemmSmem<BN>;
+    auto k = gemm_kernel<BN, EPI>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, S::TOTAL);
     if (e != cudaSuccess) return e;
-    dim3 grid(g.M / BM, g.N / BN);
-    k<<<grid, THREADS, S::TOTAL, s>>>(g);
+    int dev = 0, sms = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    const int tiles = (g.M / BM) * (g.N / BN);
+    k<<<tiles < sms ? tiles : sms, THREADS, S::TOTAL, s>>>(g);
     return cudaGetLastError();
 }
 
 template <int EPI>
 cudaError_t launch_epi(const GemmArgs& g, int bn, cudaStream_t s) {
-    if (bn == 256) return launch_bn<256, 4, EPI>(g, s);
-    return launch_bn<128, 4, EPI>(g, s);
+    if (bn == 256) return launch_bn<256, EPI>(g, s);
+    return launch_bn<128, EPI>(g, s);
 }
 
 }  // namespace
