@@ -10,7 +10,6 @@ Parameter layout (one FP32 vector): W1 (H x B), W1e (H x 4), b1 (H), W2 (H x H),
 W4 (B x H), b4 (B); B = nbins, H = hidden.
 """
 import numpy as np
-from scipy.special import erf
 
 
 def bf16(x):
@@ -21,12 +20,17 @@ def bf16(x):
     return ((u + r) & 0xFFFF0000).astype(np.uint32).view(np.float32)
 
 
+GELU_C, GELU_A = np.sqrt(2.0 / np.pi), 0.044715
+
+
 def gelu(z):
-    return 0.5 * z * (1.0 + erf(z / np.sqrt(2.0)))
+    """GELU in its tanh form, the network's activation: 0.5 z (1 + tanh(c (z + a z^3)))."""
+    return 0.5 * z * (1.0 + np.tanh(GELU_C * (z + GELU_A * z ** 3)))
 
 
 def gelu_grad(z):
-    return 0.5 * (1.0 + erf(z / np.sqrt(2.0))) + z * np.exp(-0.5 * z * z) / np.sqrt(2.0 * np.pi)
+    t = np.tanh(GELU_C * (z + GELU_A * z ** 3))
+    return 0.5 * (1.0 + t) + 0.5 * z * (1.0 - t * t) * GELU_C * (1.0 + 3.0 * GELU_A * z * z)
 
 
 def unpack(p, nbins, hidden):

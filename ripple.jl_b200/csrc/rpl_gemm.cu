@@ -4,23 +4,25 @@
 // C[M x N] = A[M x K] * B[N x K]^T, A and B row-major with K contiguous ("K-major" operands).
 // A persistent, warp-specialised kernel: one CTA per SM walks the 128 x BN output tiles (tile t and
 // t + gridDim.x, ...). Its warps split the work:
-//   warps 0-3 (producers): copy 64-wide K blocks of A and B into a STAGES-deep ring of shared-memory
-//     stages with cp.async, 128-byte swizzled so the tensor core reads them through K-major descriptors;
-//     each thread's cp.async.mbarrier.arrive.noinc arrives on the stage's `full` barrier once its copies
-//     have landed, so the producers run up to STAGES blocks ahead without waiting for their own copies;
-//   warp 4 (MMA): waits `full`, fences the stage for the async proxy, issues the block's four K = 16
-//     tcgen05.mma into one of two TMEM
-//     accumulators (double buffered across tiles), commits the stage's `empty` barrier (the producers
-//     refill it) and, after a tile's last block, the accumulator's `acc_full` barrier;
-//   warps 5-12 (epilogue, two per TMEM lane quadrant, each taking half the columns): wait `acc_full`,
-//     read their lanes with tcgen05.ld, apply the fused epilogue, store, and arrive on `acc_empty` so the
-//     MMA warp may reuse that accumulator -- the epilogue of one tile overlaps the MMAs of the next.
+//   warp 0 (producer, one thread): TMA-loads (no multicast) 64-wide K blocks of A and B into a
+//     STAGES-deep ring of shared-memory stages, 128-byte swizzled by the tensor maps so the tensor core
+//     reads them through K-major descriptors; each stage's `full` barrier completes on the bytes landed;
+//   warp 1 (MMA, one thread): waits `full`, issues the block's four K = 16 tcgen05.mma into one of two
+//     TMEM accumulators (double buffered across tiles), commits the stage's `empty` barrier (the producer
+//     refills it) and, after a tile's last block, the accumulator's `acc_full` barrier;
+//   warps 2-17 (epilogue, four per TMEM lane quadrant warp % 4, each taking a quarter of the columns):
+//     wait `acc_full`, read their lanes with tcgen05.ld, apply the fused epilogue, store, and arrive on
+//     `acc_empty` so the MMA warp may reuse that accumulator -- the epilogue of one tile overlaps the
+//     MMAs of the next.
 // Every wait is bounded and checks a shared abort flag: a wait that gives up sets bit 4 of the error word
 // and the flag, every role then leaves its loop, the copies in flight drain, TMEM is freed, and the
 // kernel returns. Requirements (checked by the host): M % 128 == 0, N % BN == 0, K % 64 == 0, 16-byte
 // aligned rows.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
+
+#include <mutex>
 
 #include "rpl_mlp.h"
 #include "rpl_umma.cuh"
@@ -30,10 +32,10 @@ namespace rpl {
 namespace {
 
 constexpr int BM = 128, BK = 64, STAGES = 4;
-constexpr int PRODUCERS = 128;                 // warps 0-3
-constexpr int MMA_WARP = 4;
-constexpr int EPILOGUE = 256;                  // warps 5-12
-constexpr int THREADS = 13 * 32;               // producers + MMA warp + epilogue warps
+constexpr int MMA_WARP = 1;
+constexpr int EPI_WARP0 = 2, EPI_WARPS = 16;   // warps 2-17
+constexpr int EPILOGUE = EPI_WARPS * 32;
+constexpr int THREADS = (EPI_WARP0 + EPI_WARPS) * 32;
 constexpr uint32_t WAIT_LIMIT = 1u << 24;
 
 template <int BN>
@@ -44,17 +46,22 @@ struct GemmSmem {
     static constexpr int TOTAL = STAGES * STAGE + 1024 /* alignment slack */;
 };
 
-__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
-__device__ __forceinline__ float gelu_grad(float z) {
-    const float cdf = 0.5f * (1.0f + erff(z * 0.70710678118654752f));
-    const float pdf = 0.39894228040143268f * expf(-0.5f * z * z);
-    return cdf + z * pdf;
+// The network's activation: GELU in its tanh form, 0.5 z (1 + tanh(c (z + a z^3))), c = sqrt(2/pi),
+// a = 0.044715, with the hardware tanh (tanh.approx.f32, relative error ~5e-4, below BF16 rounding).
+__device__ __forceinline__ float tanh_fast(float x) {
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
 }
-
-// Arrives on `bar` when every cp.async this thread issued so far has completed (the arrival counts
-// toward the barrier's expected count).
-__device__ __forceinline__ void cp_async_arrive(uint32_t bar) {
-    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(bar) : "memory");
+constexpr float GELU_C = 0.7978845608028654f, GELU_A = 0.044715f;
+__device__ __forceinline__ float gelu(float z) {
+    const float t = tanh_fast(GELU_C * fmaf(GELU_A * z, z * z, z));
+    return 0.5f * z * (1.0f + t);
+}
+__device__ __forceinline__ float gelu_grad(float z) {
+    const float z2 = z * z;
+    const float t = tanh_fast(GELU_C * fmaf(GELU_A * z, z2, z));
+    return fmaf(0.5f * z * fmaf(-t, t, 1.0f), GELU_C * fmaf(3.0f * GELU_A, z2, 1.0f), 0.5f * (1.0f + t));
 }
 
 __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
@@ -96,19 +103,35 @@ __device__ __forceinline__ void epilogue_cols(const GemmArgs& g, uint32_t trow, 
                                    v[4 * i + 2] + g.bias[col + 4 * i + 2], v[4 * i + 3] + g.bias[col + 4 * i + 3]);
         } else {
             __nv_bfloat16 h[16];
+            float u[16];
+            if (EPI == EPI_BIAS_GELU) {
+                const float4* bp = reinterpret_cast<const float4*>(g.bias + col);
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const float4 bb = __ldg(bp + i);
+                    u[4 * i] = bb.x; u[4 * i + 1] = bb.y; u[4 * i + 2] = bb.z; u[4 * i + 3] = bb.w;
+                }
+            } else {
+                const float4* pp = reinterpret_cast<const float4*>(g.pre + (int64_t)row * g.ldp + col);
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const float4 q = pp[i];
+                    u[4 * i] = q.x; u[4 * i + 1] = q.y; u[4 * i + 2] = q.z; u[4 * i + 3] = q.w;
+                }
+            }
 #pragma unroll
             for (int i = 0; i < 16; ++i) {
                 float z = v[i];
                 if (EPI == EPI_BIAS_GELU) {
-                    z += g.bias[col + i];
+                    z += u[i];
                     if (g.wextra) {
-                        const float* we = g.wextra + (int64_t)(col + i) * 4;
-                        z = fmaf(ex[0], we[0], fmaf(ex[1], we[1], fmaf(ex[2], we[2], fmaf(ex[3], we[3], z))));
+                        const float4 we = __ldg(reinterpret_cast<const float4*>(g.wextra) + col + i);
+                        z = fmaf(ex[0], we.x, fmaf(ex[1], we.y, fmaf(ex[2], we.z, fmaf(ex[3], we.w, z))));
                     }
                     if (g.out_f32) g.out_f32[(int64_t)row * g.ldo + col + i] = z;
                     z = gelu(z);
                 } else {  // EPI_GELU_BWD: upstream gradient times GELU'(pre-activation)
-                    z *= gelu_grad(g.pre[(int64_t)row * g.ldp + col + i]);
+                    z *= gelu_grad(u[i]);
                 }
                 h[i] = __float2bfloat16_rn(z);
             }
@@ -126,7 +149,8 @@ __device__ __forceinline__ void epilogue_cols(const GemmArgs& g, uint32_t trow, 
 }
 
 template <int BN, int EPI>
-__global__ void __launch_bounds__(THREADS, 1) gemm_kernel(const GemmArgs g) {
+__global__ void __launch_bounds__(THREADS, 1)
+    gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, const GemmArgs g) {
     using S = GemmSmem<BN>;
     extern __shared__ uint8_t smem_raw[];
     __shared__ uint64_t full_bar[STAGES], empty_bar[STAGES], acc_full[2], acc_empty[2];
@@ -140,7 +164,7 @@ __global__ void __launch_bounds__(THREADS, 1) gemm_kernel(const GemmArgs g) {
 
     if (tid == 0) {
         for (int s = 0; s < STAGES; ++s) {
-            umma::mbar_init(umma::smem_u32(&full_bar[s]), PRODUCERS);
+            umma::mbar_init(umma::smem_u32(&full_bar[s]), 1);
             umma::mbar_init(umma::smem_u32(&empty_bar[s]), 1);
         }
         for (int b = 0; b < 2; ++b) {
@@ -156,31 +180,27 @@ __global__ void __launch_bounds__(THREADS, 1) gemm_kernel(const GemmArgs g) {
     umma::fence_after_sync();
     const uint32_t tmem = s_tmem;
 
-    if (warp < 4) {
-        // ---- producers ----
-        int64_t gcount = 0;  // K blocks issued by this CTA so far
-        for (int t = blockIdx.x; t < tiles && !*abort_flag; t += gridDim.x) {
-            const int m0 = (t / tiles_n) * BM, n0 = (t % tiles_n) * BN;
-            for (int kb = 0; kb < KB; ++kb, ++gcount) {
-                const int s = (int)(gcount % STAGES);
-                const int64_t use = gcount / STAGES;
-                if (use > 0 && !wait_phase(umma::smem_u32(&empty_bar[s]), (uint32_t)((use - 1) & 1), abort_flag)) break;
-                const uint32_t sa = base + s * S::STAGE, sb = sa + S::A_BYTES;
-                const int k0 = kb * BK;
-#pragma unroll 4
-                for (int q = tid; q < BM * 8; q += PRODUCERS) {
-                    const int r = q >> 3, c = q & 7;
-                    umma::cp_async16(sa + r * 128 + ((c ^ (r & 7)) << 4), g.A + (int64_t)(m0 + r) * g.lda + k0 + c * 8);
+    if (warp == 0) {
+        // ---- producer (one thread): TMA loads ----
+        if (lane == 0) {
+            int64_t gcount = 0;  // K blocks issued by this CTA so far
+            for (int t = blockIdx.x; t < tiles && !*abort_flag; t += gridDim.x) {
+                const int m0 = (t / tiles_n) * BM, n0 = (t % tiles_n) * BN;
+                for (int kb = 0; kb < KB; ++kb, ++gcount) {
+                    const int s = (int)(gcount % STAGES);
+                    const int64_t use = gcount / STAGES;
+                    if (use > 0 &&
+                        !wait_phase(umma::smem_u32(&empty_bar[s]), (uint32_t)((use - 1) & 1), abort_flag))
+                        break;
+                    const uint32_t sa = base + s * S::STAGE, sb = sa + S::A_BYTES;
+                    const uint32_t bar = umma::smem_u32(&full_bar[s]);
+                    umma::mbar_arrive_expect_tx(bar, (uint32_t)S::STAGE);
+                    umma::tma_load_2d(sa, &tmA, kb * BK, m0, bar);
+                    umma::tma_load_2d(sb, &tmB, kb * BK, n0, bar);
                 }
-#pragma unroll 4
-                for (int q = tid; q < BN * 8; q += PRODUCERS) {
-                    const int r = q >> 3, c = q & 7;
-                    umma::cp_async16(sb + r * 128 + ((c ^ (r & 7)) << 4), g.B + (int64_t)(n0 + r) * g.ldb + k0 + c * 8);
-                }
-                cp_async_arrive(umma::smem_u32(&full_bar[s]));
             }
         }
-        asm volatile("cp.async.wait_all;" ::: "memory");
+        __syncwarp();
     } else if (warp == MMA_WARP) {
         // ---- MMA issue (one thread) ----
         if (lane == 0) {
@@ -199,7 +219,6 @@ __global__ void __launch_bounds__(THREADS, 1) gemm_kernel(const GemmArgs g) {
                         ok = false;
                         break;
                     }
-                    umma::fence_proxy_async();  // the producers' cp.async writes, for the tensor core's reads
                     umma::fence_after_sync();
                     const uint32_t sa = base + s * S::STAGE, sb = sa + S::A_BYTES;
 #pragma unroll
@@ -214,16 +233,16 @@ __global__ void __launch_bounds__(THREADS, 1) gemm_kernel(const GemmArgs g) {
         }
         __syncwarp();
     } else {
-        // ---- epilogue (warps 5-12: TMEM lane quadrant warp % 4, column half (warp - 5) / 4) ----
-        const int quad = warp & 3, half = (warp - 5) >> 2;
+        // ---- epilogue (warps 2-17: TMEM lane quadrant warp % 4, column quarter (warp - 2) / 4) ----
+        const int quad = warp & 3, part = (warp - EPI_WARP0) >> 2;
         int local = 0;
         for (int t = blockIdx.x; t < tiles && !*abort_flag; t += gridDim.x, ++local) {
             const int b = local & 1;
             if (!wait_phase(umma::smem_u32(&acc_full[b]), (uint32_t)((local >> 1) & 1), abort_flag)) break;
             umma::fence_after_sync();
             const int m0 = (t / tiles_n) * BM, n0 = (t % tiles_n) * BN;
-            const uint32_t trow = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(b * BN + half * (BN / 2));
-            epilogue_cols<BN / 2, EPI>(g, trow, m0 + quad * 32 + lane, n0 + half * (BN / 2));
+            const uint32_t trow = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(b * BN + part * (BN / 4));
+            epilogue_cols<BN / 4, EPI>(g, trow, m0 + quad * 32 + lane, n0 + part * (BN / 4));
             umma::fence_before_sync();
             mbar_arrive(umma::smem_u32(&acc_empty[b]));
         }
@@ -237,6 +256,38 @@ __global__ void __launch_bounds__(THREADS, 1) gemm_kernel(const GemmArgs g) {
     }
 }
 
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// The driver's tensor-map encoder, looked up once through the runtime (no link against libcuda).
+EncodeTiled encoder() {
+    static std::once_flag once;
+    static EncodeTiled fn = nullptr;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiled>(p);
+    });
+    return fn;
+}
+
+// Tensor map of a row-major BF16 matrix (rows x K, row stride ld elements): boxes of 64 K values x
+// box_rows rows, 128-byte swizzle (the layout the K-major UMMA descriptors read).
+bool encode(CUtensorMap* m, const __nv_bfloat16* base, int64_t rows, int64_t K, int64_t ld, int box_rows) {
+    EncodeTiled fn = encoder();
+    if (!fn) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
+    const cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)box_rows};
+    const cuuint32_t estr[2] = {1, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<__nv_bfloat16*>(base), dims, strides, box, estr,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 template <int BN, int EPI>
 cudaError_t launch_bn(const GemmArgs& g, cudaStream_t s) {
     using S = GemmSmem<BN>;
@@ -246,8 +297,11 @@ cudaError_t launch_bn(const GemmArgs& g, cudaStream_t s) {
     int dev = 0, sms = 0;
     if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
     if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    alignas(64) CUtensorMap ta, tb;
+    if (!encode(&ta, g.A, g.M, g.K, g.lda, BM) || !encode(&tb, g.B, g.N, g.K, g.ldb, BN))
+        return cudaErrorInvalidValue;
     const int tiles = (g.M / BM) * (g.N / BN);
-    k<<<tiles < sms ? tiles : sms, THREADS, S::TOTAL, s>>>(g);
+    k<<<tiles < sms ? tiles : sms, THREADS, S::TOTAL, s>>>(ta, tb, g);
     return cudaGetLastError();
 }
 
@@ -268,10 +322,10 @@ bool gemm_shape_ok(const GemmArgs& g, int bn) {
         case EPI_BIAS:
             return g.out_f32 && al16(g.out_f32) && g.ldo % 4 == 0 && g.ldo >= g.N && (g.epi == EPI_F32 || g.bias);
         case EPI_BIAS_GELU:
-            return g.bias && (g.out_bf16 || g.out_bf16_t) && (!g.out_bf16 || (al16(g.out_bf16) && g.ldh % 8 == 0)) &&
+            return g.bias && al16(g.bias) && (!g.wextra || al16(g.wextra)) && (g.out_bf16 || g.out_bf16_t) && (!g.out_bf16 || (al16(g.out_bf16) && g.ldh % 8 == 0)) &&
                    (!g.out_f32 || g.ldo >= g.N) && (!g.out_bf16_t || g.ldt >= g.M);
         case EPI_GELU_BWD:
-            return g.pre && g.ldp >= g.N && (g.out_bf16 || g.out_bf16_t) &&
+            return g.pre && al16(g.pre) && g.ldp % 4 == 0 && g.ldp >= g.N && (g.out_bf16 || g.out_bf16_t) &&
                    (!g.out_bf16 || (al16(g.out_bf16) && g.ldh % 8 == 0)) && (!g.out_bf16_t || g.ldt >= g.M);
         default:
             return false;

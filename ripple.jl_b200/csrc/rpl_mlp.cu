@@ -2,6 +2,7 @@
 // (rpl_gemm.cu), Adam, and the C-ABI entry points rpl_mlp_* / rpl_gemm_bf16.
 //
 // Network: x (nbins BF16 features) and e (4 FP32 extras) -> z1 = W1 x + W1e e + b1 -> h1 = GELU(z1)
+// (GELU in its tanh form, see rpl_gemm.cu)
 // -> h2 = GELU(W2 h1 + b2) -> h3 = GELU(W3 h2 + b3) -> y = W4 h3 + b4 (nbins, FP32). Rows are cells.
 // Forward GEMMs keep activations in BF16 (and, when training, their transposes and the FP32
 // pre-activations); backward: dY = 2 (y - t) / (B nbins), dW_l = dZ_l^T H_{l-1} and
