@@ -104,33 +104,52 @@ __global__ void loss_grad_kernel(const float* __restrict__ Y, const float* __res
     if (tid == 0) atomicAdd(loss, (double)red[0]);
 }
 
-// g[c] = sum_r D[r][c] (bias gradients).
+constexpr int RED_ROWS = 512;  // rows per block of the column reductions
+
+// g[c] += sum_r D[r][c] over this block's RED_ROWS rows (bias gradients; g zeroed before). Blocks of
+// 32 columns x 8 row lanes, one atomic add per column and block.
 __global__ void colsum_kernel(const bf16* __restrict__ D, int n, int cols, float* __restrict__ g) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= cols) return;
+    __shared__ float red[8][33];
+    const int c = blockIdx.x * 32 + threadIdx.x;
+    const int r0 = blockIdx.y * RED_ROWS, r1 = min(n, r0 + RED_ROWS);
     float s = 0.0f;
-    for (int r = 0; r < n; ++r) s += __bfloat162float(D[(int64_t)r * cols + c]);
-    g[c] = s;
+    if (c < cols)
+        for (int r = r0 + threadIdx.y; r < r1; r += 8) s += __bfloat162float(D[(int64_t)r * cols + c]);
+    red[threadIdx.y][threadIdx.x] = s;
+    __syncthreads();
+    if (threadIdx.y == 0 && c < cols) {
+        float t = 0.0f;
+        for (int k = 0; k < 8; ++k) t += red[k][threadIdx.x];
+        atomicAdd(g + c, t);
+    }
 }
 
-// g[h][e] = sum_r dZ[r][h] E[r][e] (gradient of the extra-input weights).
+// g[h][e] += sum_r dZ[r][h] E[r][e] over this block's rows (gradient of the extra-input weights).
 __global__ void extra_grad_kernel(const bf16* __restrict__ dZ, const float* __restrict__ E, int n, int hd,
                                   float* __restrict__ g) {
-    const int h = blockIdx.x * blockDim.x + threadIdx.x;
-    if (h >= hd) return;
+    __shared__ float red[8][4][33];
+    const int h = blockIdx.x * 32 + threadIdx.x;
+    const int r0 = blockIdx.y * RED_ROWS, r1 = min(n, r0 + RED_ROWS);
     float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
-    for (int r = 0; r < n; ++r) {
-        const float d = __bfloat162float(dZ[(int64_t)r * hd + h]);
-        const float4 e = *reinterpret_cast<const float4*>(E + (int64_t)r * 4);
-        s0 = fmaf(d, e.x, s0);
-        s1 = fmaf(d, e.y, s1);
-        s2 = fmaf(d, e.z, s2);
-        s3 = fmaf(d, e.w, s3);
+    if (h < hd)
+        for (int r = r0 + threadIdx.y; r < r1; r += 8) {
+            const float d = __bfloat162float(dZ[(int64_t)r * hd + h]);
+            const float4 e = *reinterpret_cast<const float4*>(E + (int64_t)r * 4);
+            s0 = fmaf(d, e.x, s0);
+            s1 = fmaf(d, e.y, s1);
+            s2 = fmaf(d, e.z, s2);
+            s3 = fmaf(d, e.w, s3);
+        }
+    red[threadIdx.y][0][threadIdx.x] = s0;
+    red[threadIdx.y][1][threadIdx.x] = s1;
+    red[threadIdx.y][2][threadIdx.x] = s2;
+    red[threadIdx.y][3][threadIdx.x] = s3;
+    __syncthreads();
+    if (threadIdx.y < 4 && h < hd) {
+        float t = 0.0f;
+        for (int k = 0; k < 8; ++k) t += red[k][threadIdx.y][threadIdx.x];
+        atomicAdd(g + h * 4 + threadIdx.y, t);
     }
-    g[h * 4] = s0;
-    g[h * 4 + 1] = s1;
-    g[h * 4 + 2] = s2;
-    g[h * 4 + 3] = s3;
 }
 
 __global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m1,
@@ -294,18 +313,21 @@ int batch_gradient(rpl_mlp* m, const bf16* X, const float* E, const float* T, co
         return rpl::gemm(m, g, s);
     };
     float* G = m->G;
+    MLP_CUDA(cudaMemsetAsync(G, 0, m->np * sizeof(float), s));  // the reductions below accumulate
+    const dim3 rblk(32, 8);
+    auto rgrid = [&](int cols) { return dim3((cols + 31) / 32, (B + RED_ROWS - 1) / RED_ROWS); };
     MLP_CUDA(wgrad(m->dYt, m->H3t, nb, hd, G + m->oW4));
-    colsum_kernel<<<(nb + 127) / 128, 128, 0, s>>>(m->dY, B, nb, G + m->ob4);
+    colsum_kernel<<<rgrid(nb), rblk, 0, s>>>(m->dY, B, nb, G + m->ob4);
     MLP_CUDA(dgrad(m->dY, nb, m->W4t, m->Z3, m->dZ3, m->dZ3t));
     MLP_CUDA(wgrad(m->dZ3t, m->H2t, hd, hd, G + m->oW3));
-    colsum_kernel<<<(hd + 127) / 128, 128, 0, s>>>(m->dZ3, B, hd, G + m->ob3);
+    colsum_kernel<<<rgrid(hd), rblk, 0, s>>>(m->dZ3, B, hd, G + m->ob3);
     MLP_CUDA(dgrad(m->dZ3, hd, m->W3t, m->Z2, m->dZ2, m->dZ2t));
     MLP_CUDA(wgrad(m->dZ2t, m->H1t, hd, hd, G + m->oW2));
-    colsum_kernel<<<(hd + 127) / 128, 128, 0, s>>>(m->dZ2, B, hd, G + m->ob2);
+    colsum_kernel<<<rgrid(hd), rblk, 0, s>>>(m->dZ2, B, hd, G + m->ob2);
     MLP_CUDA(dgrad(m->dZ2, hd, m->W2t, m->Z1, m->dZ1, m->dZ1t));
     MLP_CUDA(wgrad(m->dZ1t, m->Xt, hd, nb, G + m->oW1));
-    colsum_kernel<<<(hd + 127) / 128, 128, 0, s>>>(m->dZ1, B, hd, G + m->ob1);
-    extra_grad_kernel<<<(hd + 127) / 128, 128, 0, s>>>(m->dZ1, m->E, B, hd, G + m->oW1e);
+    colsum_kernel<<<rgrid(hd), rblk, 0, s>>>(m->dZ1, B, hd, G + m->ob1);
+    extra_grad_kernel<<<rgrid(hd), rblk, 0, s>>>(m->dZ1, m->E, B, hd, G + m->oW1e);
     MLP_CUDA(cudaGetLastError());
     return RPL_OK;
 }
