@@ -43,8 +43,10 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--workload", default="seamount", choices=["seamount", "hurricane", "ensemble", "learned"])
-    ap.add_argument("--train-steps", type=int, default=6000, help="Adam steps (--workload learned)")
+    ap.add_argument("--train-steps", type=int, default=40000, help="Adam steps (--workload learned)")
     ap.add_argument("--snapshots", type=int, default=40, help="training snapshots per storm run (--workload learned)")
+    ap.add_argument("--dagger", type=int, default=0,
+                    help="rounds of rows collected along learned-source runs, labelled by the plain sources (--workload learned)")
     ap.add_argument("--calm-fraction", type=float, default=0.05,
                     help="share of cells without source activity kept as training rows (--workload learned)")
     ap.add_argument("--members", type=int, default=64, help="ensemble members (--workload ensemble)")
@@ -491,37 +493,52 @@ def run_learned(args, rank, world, local_rank):
         smi_id = str(local_rank)
     n, K = args.size, args.steps
     nb, hd = 32 * 36, 512
-    net = learned.SourceNetwork(nbins=nb, hidden=hd, rows=16384, seed=5, device=local_rank)
+    net = learned.SourceNetwork(nbins=nb, hidden=hd, rows=65536, seed=5, device=local_rank)
     # 1. training rows from the plain sources
     t0 = time.perf_counter()
     storms = [dict(), dict(vmax=40.0, start=(0.3, 0.3), translation=7.0)]
     every = max(1, K // max(1, args.snapshots))
     gen = torch.Generator(device="cuda").manual_seed(7)
-    Xs, Es, Ts = [], [], []
-    for st in storms:
-        w = workloads.hurricane_swell(N=n, nsteps=K, n0_dtype=np.float32, **st)
-        m = w.model("fp32", device=local_rank)
-        for k in range(0, K, every):
-            X, E, T = learned.sample(m, net)
-            peak = T.abs().amax(1)
-            act = peak > 0.5
-            calm = (~act) & (torch.rand(peak.shape, device=peak.device, generator=gen) < args.calm_fraction)
-            keep = (act | calm).nonzero().squeeze(1)
-            Xs.append(X[keep])
-            Es.append(E[keep])
-            Ts.append(T[keep])
-            del X, E, T, peak, act, calm, keep
-            rp.time_step(m, w.dt, min(every, K - k))
-        m.close()
-    X, E, T = torch.cat(Xs), torch.cat(Es), torch.cat(Ts)
-    del Xs, Es, Ts
+    def collect(bounds=None):
+        """Rows of both storms' runs every `every` steps: plain-source runs, or (with bounds) runs driven by
+        the current network; the targets are always the plain sources' rates at the visited states."""
+        Xs, Es, Ts = [], [], []
+        for st in storms:
+            w = workloads.hurricane_swell(N=n, nsteps=K, n0_dtype=np.float32, **st)
+            m = w.model("fp32", device=local_rank)
+            if bounds is not None:
+                learned.use_learned_source(m, net, *bounds)
+            for k in range(0, K, every):
+                X, E, T = learned.sample(m, net)
+                peak = T.abs().amax(1)
+                act = peak > 0.5
+                calm = (~act) & (torch.rand(peak.shape, device=peak.device, generator=gen) < args.calm_fraction)
+                keep = (act | calm).nonzero().squeeze(1)
+                Xs.append(X[keep])
+                Es.append(E[keep])
+                Ts.append(T[keep])
+                del X, E, T, peak, act, calm, keep
+                rp.time_step(m, w.dt, min(every, K - k))
+            m.close()
+        return torch.cat(Xs), torch.cat(Es), torch.cat(Ts)
+
+    X, E, T = collect()
     torch.cuda.synchronize()
     t_data = time.perf_counter() - t0
+    # out-of-distribution bounds and output clamps from the plain-source rows only
     lo, hi = learned.input_bounds(X, E)
-    # 2. training (the library's forward/backward/Adam kernels)
+    ylo, yhi = learned.output_bounds(T)
+    # 2. training (the library's forward/backward/Adam kernels), then rounds of rows gathered along the
+    #    network's own trajectories (labelled by the plain sources) and more training
     t0 = time.perf_counter()
     losses = learned.train(net, X, E, T, steps=args.train_steps, batch=16384, lr=1e-3,
                            weights=learned.row_weights(T), log_every=max(1, args.train_steps // 4))
+    for r in range(args.dagger):
+        X2, E2, T2 = collect((lo, hi, ylo, yhi))
+        X, E, T = torch.cat([X, X2]), torch.cat([E, E2]), torch.cat([T, T2])
+        del X2, E2, T2
+        losses += learned.train(net, X, E, T, steps=args.train_steps // 2, batch=16384, lr=5e-4, seed=r + 1,
+                                weights=learned.row_weights(T), log_every=max(1, args.train_steps // 4))
     torch.cuda.synchronize()
     t_train = time.perf_counter() - t0
     rows = int(X.shape[0])
@@ -532,12 +549,12 @@ def run_learned(args, rank, world, local_rank):
     for mode in ("plain", "learned"):
         warm = w.model("fp32", device=local_rank)     # warm-up on a throwaway copy
         if mode == "learned":
-            learned.use_learned_source(warm, net, lo, hi)
+            learned.use_learned_source(warm, net, lo, hi, ylo, yhi)
         rp.time_step(warm, w.dt, args.warmup)
         warm.close()
         m = w.model("fp32", device=local_rank)
         if mode == "learned":
-            learned.use_learned_source(m, net, lo, hi)
+            learned.use_learned_source(m, net, lo, hi, ylo, yhi)
         lib, h = m._lib, m.handle
         stream = torch.cuda.Stream(device=local_rank)
         _lib.check(lib.rpl_set_stream(h, _lib.ctypes.c_void_p(stream.cuda_stream)))
@@ -601,7 +618,8 @@ def run_learned(args, rank, world, local_rank):
                        "mean_spectrum_relL2_vs_plain": dS,
                        "total_action_rel_diff": abs(a["total"] - b["total"]) / b["total"],
                        "fallback_cells_last_stage": a["fallback"], "cells": P,
-                       "training_rows": rows, "training_steps": args.train_steps, "training_s": t_train,
+                       "training_rows": rows, "training_steps": args.train_steps * (2 + args.dagger) // 2,
+                       "dagger_rounds": args.dagger, "training_s": t_train,
                        "data_generation_s": t_data, "losses": losses,
                        "mlp_forward_ms_per_stage": fwd_ms, "mlp_forward_tflops": flops / fwd_ms / 1e9,
                        "mlp_tensor_frac": flops / fwd_ms / 1e9 / bf16_peak, "bf16_peak_tflops": bf16_peak,

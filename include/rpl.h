@@ -288,8 +288,11 @@ int rpl_gemm_bf16(const void* A, const void* B, float* C, int32_t M, int32_t N, 
  * (c = i + Nx j) row c of X, E and T (device arrays of Nx*Ny rows; T = asinh(rate / target_scale)). */
 int rpl_learned_sample(rpl_handle* h, const rpl_mlp* m, void* X, float* E, float* T);
 /* Use `m` (NULL: back to the plain sources) for the handle's sources. lo, hi: host arrays of nbins + 4
- * input bounds; a cell with any input outside [lo, hi] uses the plain sources. */
-int rpl_set_learned_source(rpl_handle* h, rpl_mlp* m, const float* lo, const float* hi);
+ * input bounds; a cell with any input outside [lo, hi] uses the plain sources. ylo, yhi (nbins each, or
+ * both NULL): bounds the network outputs are clamped to before they become rates (the range of the
+ * training targets keeps an extrapolating network from producing rates no source ever had). */
+int rpl_set_learned_source(rpl_handle* h, rpl_mlp* m, const float* lo, const float* hi, const float* ylo,
+                           const float* yhi);
 /* Network outputs y of the most recent stage (host, Nx*Ny rows of nbins, row c = cell i + Nx j). */
 int rpl_learned_outputs(rpl_handle* h, float* Y);
 /* Cells that fell back to the plain sources in the most recent stage. */

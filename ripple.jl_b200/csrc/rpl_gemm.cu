@@ -98,9 +98,13 @@ __device__ __forceinline__ void epilogue_cols(const GemmArgs& g, uint32_t trow, 
         } else if (EPI == EPI_BIAS) {
             float4* o = reinterpret_cast<float4*>(g.out_f32 + (int64_t)row * g.ldo + col);
 #pragma unroll
-            for (int i = 0; i < 4; ++i)
-                o[i] = make_float4(v[4 * i] + g.bias[col + 4 * i], v[4 * i + 1] + g.bias[col + 4 * i + 1],
-                                   v[4 * i + 2] + g.bias[col + 4 * i + 2], v[4 * i + 3] + g.bias[col + 4 * i + 3]);
+            for (int i = 0; i < 16; ++i) v[i] += g.bias[col + i];
+            if (g.clamp_lo) {
+#pragma unroll
+                for (int i = 0; i < 16; ++i) v[i] = fminf(fmaxf(v[i], g.clamp_lo[col + i]), g.clamp_hi[col + i]);
+            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i) o[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
         } else {
             __nv_bfloat16 h[16];
             float u[16];
@@ -320,7 +324,8 @@ bool gemm_shape_ok(const GemmArgs& g, int bn) {
     switch (g.epi) {
         case EPI_F32:
         case EPI_BIAS:
-            return g.out_f32 && al16(g.out_f32) && g.ldo % 4 == 0 && g.ldo >= g.N && (g.epi == EPI_F32 || g.bias);
+            return g.out_f32 && al16(g.out_f32) && g.ldo % 4 == 0 && g.ldo >= g.N && (g.epi == EPI_F32 || g.bias) &&
+                   (!g.clamp_lo) == (!g.clamp_hi);
         case EPI_BIAS_GELU:
             return g.bias && al16(g.bias) && (!g.wextra || al16(g.wextra)) && (g.out_bf16 || g.out_bf16_t) && (!g.out_bf16 || (al16(g.out_bf16) && g.ldh % 8 == 0)) &&
                    (!g.out_f32 || g.ldo >= g.N) && (!g.out_bf16_t || g.ldt >= g.M);

@@ -129,6 +129,7 @@ struct Handle {
     unsigned int* d_lflag = nullptr;  // per cell: inputs outside the bounds -> plain sources
     float* d_lbounds = nullptr;    // lo[nbins + 4], hi[nbins + 4]
     int64_t lrows = 0;
+    bool lclamp = false;           // clamp the network outputs to the output bounds
     bool currents_set = false;
     // sources
     rpl_sources src{};

@@ -130,7 +130,9 @@ cudaError_t launch_learned_stage_prep(const Handle& h, const void* Nin, cudaStre
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (h.src.stress_cap && (e = launch_stress_factor(h, Nin, s, h.d_lflag)) != cudaSuccess) return e;
     const int nb = mlp_nbins(h.learned);
-    return mlp_forward(h.learned, (const bf16*)h.d_lx, nb, h.d_le, h.lrows, h.d_lr, nb, false, s, h.d_err);
+    const float* ylo = h.lclamp ? h.d_lbounds + 2 * (nb + 4) : nullptr;
+    return mlp_forward(h.learned, (const bf16*)h.d_lx, nb, h.d_le, h.lrows, h.d_lr, nb, false, s, h.d_err, ylo,
+                       ylo ? ylo + nb : nullptr);
 }
 
 void free_learned(Handle* h) {
@@ -173,7 +175,8 @@ int rpl_learned_sample(rpl_handle* hh, const rpl_mlp* m, void* X, float* E, floa
     return RPL_OK;
 }
 
-int rpl_set_learned_source(rpl_handle* hh, rpl_mlp* m, const float* lo, const float* hi) {
+int rpl_set_learned_source(rpl_handle* hh, rpl_mlp* m, const float* lo, const float* hi, const float* ylo,
+                           const float* yhi) {
     if (!hh) return rpl::lfail(RPL_ERR_ARGUMENT, "null handle");
     Handle* h = reinterpret_cast<Handle*>(hh);
     cudaError_t e = cudaSetDevice(h->device);
@@ -187,21 +190,30 @@ int rpl_set_learned_source(rpl_handle* hh, rpl_mlp* m, const float* lo, const fl
     const int nb = rpl::mlp_nbins(m);
     for (int i = 0; i < nb + 4; ++i)
         if (!(lo[i] <= hi[i])) return rpl::lfail(RPL_ERR_ARGUMENT, "input bounds need lo <= hi");
+    if ((ylo == nullptr) != (yhi == nullptr)) return rpl::lfail(RPL_ERR_ARGUMENT, "give both output bounds or neither");
+    if (ylo)
+        for (int i = 0; i < nb; ++i)
+            if (!(ylo[i] <= yhi[i])) return rpl::lfail(RPL_ERR_ARGUMENT, "output bounds need ylo <= yhi");
     const int64_t rows = (h->cells + 127) / 128 * 128;
-    const size_t need = rows * nb * (2 + 4) + rows * 16 + h->cells * 4 + (size_t)2 * (nb + 4) * 4;
+    const size_t nbound = (size_t)2 * (nb + 4) + 2 * nb;  // input lo, hi, output lo, hi
+    const size_t need = rows * nb * (2 + 4) + rows * 16 + h->cells * 4 + nbound * 4;
     if (h->desc.memory_limit_bytes > 0 && h->bytes + (int64_t)need > h->desc.memory_limit_bytes)
         return rpl::lfail(RPL_ERR_OOM, "the learned source's buffers would exceed memory_limit_bytes");
     auto al = [&](auto** p, size_t bytes) { return cudaMalloc((void**)p, bytes); };
     if ((e = al(&h->d_lx, rows * nb * 2)) != cudaSuccess || (e = al(&h->d_le, rows * 16)) != cudaSuccess ||
         (e = al(&h->d_lr, rows * nb * 4)) != cudaSuccess ||
         (e = al(&h->d_lflag, h->cells * sizeof(unsigned int))) != cudaSuccess ||
-        (e = al(&h->d_lbounds, (size_t)2 * (nb + 4) * 4)) != cudaSuccess) {
+        (e = al(&h->d_lbounds, nbound * 4)) != cudaSuccess) {
         rpl::free_learned(h);
         return rpl::lfail(e == cudaErrorMemoryAllocation ? RPL_ERR_OOM : RPL_ERR_CUDA, "learned-source buffers");
     }
-    std::vector<float> b(2 * (nb + 4));
+    std::vector<float> b(nbound, 0.0f);
     std::copy(lo, lo + nb + 4, b.begin());
     std::copy(hi, hi + nb + 4, b.begin() + nb + 4);
+    if (ylo) {
+        std::copy(ylo, ylo + nb, b.begin() + 2 * (nb + 4));
+        std::copy(yhi, yhi + nb, b.begin() + 2 * (nb + 4) + nb);
+    }
     if ((e = cudaMemsetAsync(h->d_lx, 0, rows * nb * 2, h->stream)) != cudaSuccess ||
         (e = cudaMemsetAsync(h->d_le, 0, rows * 16, h->stream)) != cudaSuccess ||
         (e = cudaMemsetAsync(h->d_lflag, 0, h->cells * sizeof(unsigned int), h->stream)) != cudaSuccess ||
@@ -212,6 +224,7 @@ int rpl_set_learned_source(rpl_handle* hh, rpl_mlp* m, const float* lo, const fl
     }
     h->learned = m;
     h->lrows = rows;
+    h->lclamp = ylo != nullptr;
     return RPL_OK;
 }
 

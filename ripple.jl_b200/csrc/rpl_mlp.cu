@@ -231,7 +231,7 @@ static cudaError_t gemm(rpl_mlp* m, GemmArgs g, cudaStream_t s) {
 // Forward over n rows (n % 128 == 0) of X (row stride ldx) / E, output rows of Y (row stride ldy). With
 // `train` (n <= R) the pre-activations and transposed activations for the backward pass are kept.
 cudaError_t mlp_forward(rpl_mlp* m, const bf16* X, int64_t ldx, const float* E, int64_t n, float* Y, int64_t ldy,
-                        bool train, cudaStream_t s, unsigned int* err) {
+                        bool train, cudaStream_t s, unsigned int* err, const float* ylo, const float* yhi) {
     const int nb = m->nb, hd = m->hd, R = m->R;
     auto run = [&](GemmArgs g) {
         g.err = err ? err : m->d_err;
@@ -262,7 +262,7 @@ cudaError_t mlp_forward(rpl_mlp* m, const bf16* X, int64_t ldx, const float* E, 
         // output layer
         GemmArgs o{};
         o.M = rows; o.epi = EPI_BIAS; o.A = m->H3; o.lda = hd; o.B = m->W4b; o.ldb = hd; o.K = hd; o.N = nb;
-        o.bias = m->P + m->ob4; o.out_f32 = Y + r0 * ldy; o.ldo = ldy;
+        o.bias = m->P + m->ob4; o.out_f32 = Y + r0 * ldy; o.ldo = ldy; o.clamp_lo = ylo; o.clamp_hi = yhi;
         if ((e = run(o)) != cudaSuccess) return e;
     }
     return cudaSuccess;

@@ -34,6 +34,8 @@ struct GemmArgs {
     int64_t ldt;
     const float* pre;        // M x N pre-activations (EPI_GELU_BWD), row stride ldp
     int64_t ldp;
+    const float* clamp_lo;   // EPI_BIAS: per-column bounds the output is clamped to (both or neither)
+    const float* clamp_hi;
     unsigned int* err;       // bit 4: a bounded wait gave up
 };
 
@@ -42,7 +44,9 @@ cudaError_t launch_gemm(const GemmArgs& g, int bn, cudaStream_t s);
 
 // Network forward over n rows (n % 128 == 0): X (row stride ldx) and E -> Y (row stride ldy), on stream s;
 // GEMM wait timeouts set bit 4 of *err (the network's own error word when err is NULL).
+// ylo, yhi (nbins each, optional): bounds the outputs are clamped to.
 cudaError_t mlp_forward(rpl_mlp* m, const __nv_bfloat16* X, int64_t ldx, const float* E, int64_t n, float* Y,
-                        int64_t ldy, bool train, cudaStream_t s, unsigned int* err);
+                        int64_t ldy, bool train, cudaStream_t s, unsigned int* err, const float* ylo = nullptr,
+                        const float* yhi = nullptr);
 
 }  // namespace rpl

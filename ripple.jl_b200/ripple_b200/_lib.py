@@ -127,7 +127,8 @@ _SIGNATURES = {
                                      ctypes.c_void_p]),
     "rpl_learned_sample": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                           ctypes.c_void_p]),
-    "rpl_set_learned_source": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "rpl_set_learned_source": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                              ctypes.c_void_p, ctypes.c_void_p]),
     "rpl_learned_outputs": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "rpl_learned_fallback_cells": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(_i64)]),
     "rpl_last_error": (ctypes.c_char_p, []),

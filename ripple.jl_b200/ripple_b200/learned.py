@@ -114,19 +114,35 @@ def sample(model, net, out=None):
     return X, E, T
 
 
-def use_learned_source(model, net, lo=None, hi=None):
+def use_learned_source(model, net, lo=None, hi=None, ylo=None, yhi=None):
     """Replace the model's plain sources by `net` (None: back to the plain sources). lo, hi: input bounds
-    (nbins + 4 values); a cell with any input outside them uses the plain sources."""
+    (nbins + 4 values); a cell with any input outside them uses the plain sources. ylo, yhi (optional,
+    nbins values): the network's outputs are clamped to them (see output_bounds)."""
     if net is None:
-        check(model._lib.rpl_set_learned_source(model.handle, None, None, None))
+        check(model._lib.rpl_set_learned_source(model.handle, None, None, None, None, None))
         return
     lo = np.ascontiguousarray(lo, dtype=np.float32)
     hi = np.ascontiguousarray(hi, dtype=np.float32)
     if lo.size != net.nbins + 4 or hi.size != net.nbins + 4:
         raise ArgumentError("bounds need nbins + 4 values")
+    yp = [None, None]
+    if ylo is not None:
+        ylo = np.ascontiguousarray(ylo, dtype=np.float32)
+        yhi = np.ascontiguousarray(yhi, dtype=np.float32)
+        if ylo.size != net.nbins or yhi.size != net.nbins:
+            raise ArgumentError("output bounds need nbins values")
+        yp = [ctypes.c_void_p(ylo.ctypes.data), ctypes.c_void_p(yhi.ctypes.data)]
     check(model._lib.rpl_set_learned_source(model.handle, net.handle, ctypes.c_void_p(lo.ctypes.data),
-                                            ctypes.c_void_p(hi.ctypes.data)))
-    model._learned_keep = (net, lo, hi)
+                                            ctypes.c_void_p(hi.ctypes.data), *yp))
+    model._learned_keep = (net, lo, hi, ylo, yhi)
+
+
+def output_bounds(T, margin=0.1):
+    """Per-output [lo, hi] of the training targets T (network output units), widened by `margin` of the
+    range."""
+    lo, hi = T.amin(0), T.amax(0)
+    pad = margin * (hi - lo)
+    return (lo - pad).cpu().numpy(), (hi + pad).cpu().numpy()
 
 
 def outputs(model, nbins):
