@@ -119,14 +119,27 @@ typedef struct rpl_sources {
 int rpl_create(const rpl_desc* desc, rpl_handle** out);
 int rpl_destroy(rpl_handle* h);
 
-/* Replaces build_coupling(PrescribedVelocities) + update_coupling! (lagrangian_velocities.jl:434-440,
+/* Replaces build_coupling(PrescribedVelocities) + update_coupling! (lagrangian_velocities.jl:286-292,
  * current_coupling.jl:127-138): Q-transform Doppler velocity U and dU/dkappa on the device
  * (doppler_velocity.jl:45-82, q_kernel.jl:60-116) and their periodic gradients
  * (wave_current_refraction.jl:7-39). u, v: (Nx,Ny,Nz) x fastest; z_faces: Nz+1 increasing;
- * q_depth: column depth for the projection (grid depth for InfiniteDepth, lagrangian_velocities.jl:340-342). */
+ * q_depth: column depth for the projection (grid depth for InfiniteDepth, lagrangian_velocities.jl:192-194). */
 int rpl_set_currents(rpl_handle* h, int64_t Nz, const double* z_faces,
                      int32_t q_depth_kind, double q_depth_constant, const double* q_depth_field,
                      const double* u, const double* v, double small_mu);
+/* Replaces build_coupling(PseudomomentumVelocities) + CWCMPseudomomentumCoupling
+ * (lagrangian_velocities.jl:294-311, current_coupling.jl:93-118): builds the vertical overlap tables of
+ * the Q transform (pseudomomentum.jl:68-121; one Nk x Nk pair for RPL_DEPTH_CONSTANT, one per (i,j) for
+ * RPL_DEPTH_FIELD) and the first-moment measures (polar_wavevector_grid.jl:73-110). From then on every
+ * RK3 stage and rpl_tendency recompute the Doppler velocity from that stage's action
+ * (current_coupling.jl:140-143, tendencies.jl:103-107, pseudomomentum.jl:123-138,316-342). Needs
+ * RPL_TRANSPORT_REFRACTION and Nk <= 256; z_faces: Nz+1 increasing; q_depth as for rpl_set_currents.
+ * A later rpl_set_currents switches back to prescribed currents. The coupling starts at zero. */
+int rpl_set_pseudomomentum(rpl_handle* h, int64_t Nz, const double* z_faces, int32_t q_depth_kind,
+                           double q_depth_constant, const double* q_depth_field, double small_mu);
+/* Replaces update_coupling!(model) (current_coupling.jl:140-148): with pseudomomentum velocities,
+ * recomputes the coupling from the current action; with prescribed currents, nothing to do. */
+int rpl_update_coupling(rpl_handle* h);
 /* Copies the cached coupling fields to the host (coupling.Ux/Uy/dUxdkappa/dUydkappa and
  * coupling.Ux_x/Ux_y/Uy_x/Uy_y of current_coupling.jl:19-39); any pointer may be NULL. (Nx,Ny,Nk) each. */
 int rpl_get_coupling(rpl_handle* h, double* Ux, double* Uy, double* dUxdk, double* dUydk,

@@ -38,7 +38,8 @@ class OraModel(ctypes.Structure):
                 ("holland", OraHolland), ("wind_U10", _dp), ("wind_theta", _dp), ("beta_max", _d),
                 ("z_alpha", _d), ("p_in", _d), ("alpha0", _d), ("rho_air", _d), ("rho_water", _d),
                 ("von_karman", _d), ("gravity", _d), ("has_dissipation", _i32), ("C_ds", _d), ("B_r", _d),
-                ("ds_p", _d), ("sigma_power", _d), ("ds_gravity", _d)]
+                ("ds_p", _d), ("sigma_power", _d), ("ds_gravity", _d), ("pm_mode", _i32), ("pm_per_cell", _i32),
+                ("pm_overlap", _dp), ("pm_kx", _dp), ("pm_ky", _dp)]
 
 
 def build():
@@ -78,6 +79,12 @@ def lib():
         L.ora_stress_factor.argtypes = [ctypes.POINTER(OraModel), _dp, _d, _dp]
         L.ora_rk3_step.argtypes = [ctypes.POINTER(OraModel), _dp, _d, _i64, _dp]
         L.ora_diagnostics.argtypes = [ctypes.POINTER(OraModel), _dp, _dp, _dp, _dp, _dp, _dp]
+        L.ora_first_moment_measures.argtypes = [_i64, _i64, _dp, _dp, _dp, _dp]
+        L.ora_pm_overlap_tables.argtypes = [_i64, _i64, _i64, _dp, _i64, _dp, _dp, _d, _d, _dp, _dp]
+        L.ora_pm_doppler_velocity.argtypes = [_i64, _i64, _i64, _i64, _dp, _i32, _dp, _dp, _dp, _dp,
+                                              _dp, _dp, _dp, _dp]
+        L.ora_pm_cells.argtypes = [_i64, _i64, _i64, _i64, _dp, _i64, _dp, _dp, _d, _dp, _dp, _dp, _d, _i32,
+                                   _dp, _dp]
         L.ora_num_threads.restype = ctypes.c_int
         L.ora_set_num_threads.argtypes = [ctypes.c_int]
         _lib = L
@@ -178,7 +185,10 @@ class Oracle:
         m.cg_x, m.cg_y = p(cgx), p(cgy)
         if w.velocities is not None:
             m.transport = TRANSPORT_REFRACTION
-            self._set_currents(w)
+            if type(w.velocities).__name__ == "PseudomomentumVelocities":
+                self._set_pseudomomentum(w)
+            else:
+                self._set_currents(w)
         elif w.horizontal_advection is not None:
             m.transport = TRANSPORT_INTRINSIC
         else:
@@ -210,6 +220,85 @@ class Oracle:
                                 p(self.U["Ux_x"]), p(self.U["Ux_y"]), p(self.U["Uy_x"]), p(self.U["Uy_y"]))
         m.Ux, m.Uy = p(self.U["Ux"]), p(self.U["Uy"])
         m.Uxx, m.Uxy, m.Uyx, m.Uyy = p(self.U["Ux_x"]), p(self.U["Ux_y"]), p(self.U["Uy_x"]), p(self.U["Uy_y"])
+
+    def _q_faces_and_depth(self, w, q_grid, Nz=None, surface_spacing=None, stretch=2.0):
+        """Q-transform z faces and projection depth (lagrangian_velocities.jl:192-225,294-311)."""
+        g = w.grid
+        depth = w.depth
+        infinite = type(depth).__name__ == "InfiniteDepth"
+        if q_grid is None and not g.has_flat_vertical():
+            q_grid = g
+        if q_grid is not None:
+            zf = f64(q_grid.zfaces())
+        else:
+            if infinite:
+                raise ValueError("Flat wave grids need a finite depth or a q_grid")
+            H = float(depth) if np.isscalar(depth) else float(np.max(depth))
+            dz = 1.0 / (20.0 * float(np.max(self._k))) if surface_spacing is None else float(surface_spacing)
+            if Nz is None:
+                Nz = max(16, math.ceil((H / dz) ** (1.0 / stretch)))
+            zf = f64([-H * (1.0 - k / Nz) ** stretch for k in range(Nz + 1)])
+        if infinite:
+            return zf, None, float(zf[-1] - zf[0])
+        if np.isscalar(depth):
+            return zf, None, float(depth)
+        return zf, xfast(depth), 0.0
+
+    def _set_pseudomomentum(self, w):
+        """PseudomomentumVelocities: overlap and moment tables (current_coupling.jl:93-118); the velocity
+        itself is recomputed from the action inside every tendency."""
+        L = lib()
+        v = w.velocities
+        zf, dfield, dconst = self._q_faces_and_depth(w, v.q_grid, v.Nz, v.surface_spacing,
+                                                     float(v.vertical_stretching))
+        Nk, Np = self.Nk, self.Np
+        kx, ky = np.empty(Nk * Np), np.empty(Nk * Np)
+        L.ora_first_moment_measures(Nk, Np, p(self._kf), p(self._pf), p(kx), p(ky))
+        cols = 1 if dfield is None else self.Nx * self.Ny
+        ov, dov = np.empty(cols * Nk * Nk), np.empty(cols * Nk * Nk)
+        L.ora_pm_overlap_tables(self.Nx, self.Ny, Nk, p(self._k), len(zf) - 1, p(zf), p(dfield), dconst, 1e-6,
+                                p(ov), p(dov))
+        self.pm = dict(zfaces=zf, depth_field=dfield, depth=dconst, kx=kx, ky=ky, overlap=ov,
+                       derivative_overlap=dov, per_cell=int(dfield is not None))
+        m = self.m
+        m.pm_mode, m.pm_per_cell = 1, self.pm["per_cell"]
+        m.pm_overlap, m.pm_kx, m.pm_ky = p(ov), p(kx), p(ky)
+
+    def pm_velocity(self, N):
+        """Pseudomomentum Doppler velocity of the action N (pseudomomentum.jl:123-138,316-342):
+        Ux, Uy, dUxdkappa, dUydkappa as (Nx, Ny, Nk) arrays."""
+        q = self.pm
+        N = xfast(N)
+        shape = (self.Nx, self.Ny, self.Nk)
+        outs = [np.empty(shape, order="F") for _ in range(4)]
+        lib().ora_pm_doppler_velocity(self.Nx, self.Ny, self.Nk, self.Np, p(N), q["per_cell"], p(q["overlap"]),
+                                      p(q["derivative_overlap"]), p(q["kx"]), p(q["ky"]), *[p(o) for o in outs])
+        return dict(zip(("Ux", "Uy", "dUxdkappa", "dUydkappa"), outs))
+
+    def pm_cells(self, N, cell_average=True):
+        """Pseudomomentum per Q-grid cell (pseudomomentum.jl:173-210,380-410): px, py as (Nx, Ny, Nz)."""
+        q = self.pm
+        N = xfast(N)
+        Nz = len(q["zfaces"]) - 1
+        px, py = np.empty((self.Nx, self.Ny, Nz), order="F"), np.empty((self.Nx, self.Ny, Nz), order="F")
+        lib().ora_pm_cells(self.Nx, self.Ny, self.Nk, self.Np, p(N), Nz, p(q["zfaces"]), p(q["depth_field"]),
+                           q["depth"], p(self._k), p(q["kx"]), p(q["ky"]), 1e-6, int(cell_average), p(px), p(py))
+        return px, py
+
+    def doppler_of(self, u, v):
+        """Q-transform Doppler velocity of a current profile (u, v) on the pseudomomentum Q grid
+        (doppler_velocity.jl:45-82): Ux, Uy, dUxdkappa, dUydkappa."""
+        q = self.pm
+        L = lib()
+        Nz = len(q["zfaces"]) - 1
+        u, v = xfast(u), xfast(v)
+        shape = (self.Nx, self.Ny, self.Nk)
+        outs = [np.empty(shape, order="F") for _ in range(4)]
+        L.ora_doppler_velocity(self.Nx, self.Ny, Nz, self.Nk, p(u), p(v), p(q["depth_field"]), q["depth"], p(self._k),
+                               p(q["zfaces"]), 1e-6, 0, p(outs[0]), p(outs[1]))
+        L.ora_doppler_velocity(self.Nx, self.Ny, Nz, self.Nk, p(u), p(v), p(q["depth_field"]), q["depth"], p(self._k),
+                               p(q["zfaces"]), 1e-6, 1, p(outs[2]), p(outs[3]))
+        return dict(zip(("Ux", "Uy", "dUxdkappa", "dUydkappa"), outs))
 
     def _set_sources(self, s):
         m = self.m

@@ -219,6 +219,108 @@ void ora_current_gradients(int64_t Nx, int64_t Ny, int64_t Nk, const double* Ux,
             }
 }
 
+/* -------------------------------------------------------- pseudomomentum self-coupling */
+
+/* src/CoordinateGrids/polar_wavevector_grid.jl:73-99,107-110 (spectral_first_moment_measures):
+ * kx = (k2^3 - k1^3)/3 * (sin p2 - sin p1), ky = (k2^3 - k1^3)/3 * (cos p1 - cos p2), (Nk,Np) m fastest. */
+void ora_first_moment_measures(int64_t Nk, int64_t Np, const double* kf, const double* pf, double* kx,
+                               double* ky) {
+    for (int64_t n = 0; n < Np; ++n)
+        for (int64_t m = 0; m < Nk; ++m) {
+            const double k1 = kf[m], k2 = kf[m + 1], p1 = pf[n], p2 = pf[n + 1];
+            const double radial = (k2 * k2 * k2 - k1 * k1 * k1) / 3.0;
+            kx[m + Nk * n] = radial * (std::sin(p2) - std::sin(p1));
+            ky[m + Nk * n] = radial * (std::cos(p1) - std::cos(p2));
+        }
+}
+
+/* src/Coupling/pseudomomentum.jl:68-121: overlap[t,s] = sum_k Qcell(kappa_t) * Qcell(kappa_s) / |dz_k| and
+ * derivative_overlap[t,s] = sum_k dQcell/dkappa(kappa_t) * Qcell(kappa_s) / |dz_k|, sequential in k, with the
+ * host Q forms (q_kernel.jl:18-58). depth_field NULL: (Nk,Nk) tables, target fastest; else per-column tables
+ * (Nx,Ny,Nk,Nk), x fastest. */
+void ora_pm_overlap_tables(int64_t Nx, int64_t Ny, int64_t Nk, const double* kappa, int64_t Nz,
+                           const double* zf, const double* depth_field, double depth_scalar, double small_mu,
+                           double* overlap, double* doverlap) {
+    const int64_t cols = depth_field ? Nx * Ny : 1;
+#pragma omp parallel for schedule(static)
+    for (int64_t c = 0; c < cols; ++c) {
+        const double d = depth_field ? depth_field[c] : depth_scalar;
+        for (int64_t sm = 0; sm < Nk; ++sm)
+            for (int64_t tm = 0; tm < Nk; ++tm) {
+                double total = 0.0, dtotal = 0.0;
+                for (int64_t k = 0; k < Nz; ++k) {
+                    const double z1 = zf[k], z2 = zf[k + 1], dz = std::fabs(z2 - z1);
+                    const double sw = ora_q_cell_integral(kappa[sm], z1, z2, d, small_mu);
+                    const double tw = ora_q_cell_integral(kappa[tm], z1, z2, d, small_mu);
+                    const double td = ora_q_cell_integral_kappa_derivative(kappa[tm], z1, z2, d, small_mu);
+                    total += tw * sw / dz;
+                    dtotal += td * sw / dz;
+                }
+                const int64_t e = tm + Nk * sm;
+                overlap[c + cols * e] = total;
+                doverlap[c + cols * e] = dtotal;
+            }
+    }
+}
+
+/* src/Coupling/pseudomomentum.jl:123-138,316-342: per (i,j,t) U = sum over n (outer) and source s (inner)
+ * of overlap[t,s] * N[i,j,s,n] * kx_measure[s,n] (ky for Uy, derivative_overlap for dU/dkappa). N and the
+ * outputs x fastest; per_cell selects the (Nx,Ny,Nk,Nk) tables. */
+void ora_pm_doppler_velocity(int64_t Nx, int64_t Ny, int64_t Nk, int64_t Np, const double* N, int32_t per_cell,
+                             const double* overlap, const double* doverlap, const double* kx, const double* ky,
+                             double* Ux, double* Uy, double* dUx, double* dUy) {
+    const int64_t P = Nx * Ny, cols = per_cell ? P : 1;
+#pragma omp parallel for schedule(static)
+    for (int64_t c = 0; c < P; ++c) {
+        const int64_t tc = per_cell ? c : 0;
+        for (int64_t tm = 0; tm < Nk; ++tm) {
+            double ax = 0.0, ay = 0.0, dax = 0.0, day = 0.0;
+            for (int64_t n = 0; n < Np; ++n)
+                for (int64_t sm = 0; sm < Nk; ++sm) {
+                    const double a = N[c + P * (sm + Nk * n)];
+                    const double q = overlap[tc + cols * (tm + Nk * sm)];
+                    const double dq = doverlap ? doverlap[tc + cols * (tm + Nk * sm)] : 0.0;
+                    ax += q * a * kx[sm + Nk * n];
+                    ay += q * a * ky[sm + Nk * n];
+                    dax += dq * a * kx[sm + Nk * n];
+                    day += dq * a * ky[sm + Nk * n];
+                }
+            const int64_t o = c + P * tm;
+            if (Ux) Ux[o] = ax;
+            if (Uy) Uy[o] = ay;
+            if (dUx) dUx[o] = dax;
+            if (dUy) dUy[o] = day;
+        }
+    }
+}
+
+/* src/Coupling/pseudomomentum.jl:173-210,380-410 (compute_pseudomomentum_cell_integrals / _averages):
+ * p[i,j,k] = sum over n (outer), m (inner) of Qcell_kernel(kappa_m, z_k, z_k+1, d) * N * k_measure, divided
+ * by |dz_k| when cell_average. Outputs (Nx,Ny,Nz) x fastest. */
+void ora_pm_cells(int64_t Nx, int64_t Ny, int64_t Nk, int64_t Np, const double* N, int64_t Nz, const double* zf,
+                  const double* depth_field, double depth_scalar, const double* kappa, const double* kx,
+                  const double* ky, double small_mu, int32_t cell_average, double* px, double* py) {
+    const int64_t P = Nx * Ny;
+#pragma omp parallel for schedule(static)
+    for (int64_t c = 0; c < P; ++c) {
+        const double d = depth_field ? depth_field[c] : depth_scalar;
+        for (int64_t k = 0; k < Nz; ++k) {
+            const double z1 = zf[k], z2 = zf[k + 1];
+            double ax = 0.0, ay = 0.0;
+            for (int64_t n = 0; n < Np; ++n)
+                for (int64_t m = 0; m < Nk; ++m) {
+                    const double q = ora_q_cell_integral_kernel(kappa[m], z1, z2, d, small_mu);
+                    const double a = N[c + P * (m + Nk * n)];
+                    ax += q * a * kx[m + Nk * n];
+                    ay += q * a * ky[m + Nk * n];
+                }
+            const double scale = cell_average ? 1.0 / std::fabs(z2 - z1) : 1.0;
+            px[c + P * k] = ax * scale;
+            py[c + P * k] = ay * scale;
+        }
+    }
+}
+
 /* -------------------------------------------------------- spectral grid */
 
 /* src/CoordinateGrids/spectral_grids.jl:4-27 */
@@ -572,7 +674,25 @@ static void add_sources(const ora_model* M, const double* N, double t, double* G
 /* src/Models/tendencies.jl:28-41,82-101 (dispatch) */
 void ora_tendency(const ora_model* M, const double* N, double t, int32_t with_sources, double* G) {
     const int64_t total = M->Nx * M->Ny * M->Nk * M->Np;
-    if (M->transport == ORA_TRANSPORT_REFRACTION) refraction_tendency(M, N, G);
+    if (M->transport == ORA_TRANSPORT_REFRACTION && M->pm_mode) {
+        /* PseudomomentumVelocities: the coupling is refreshed from the stage's action before every
+         * tendency (tendencies.jl:103-107, current_coupling.jl:140-143), then the gradients
+         * (wave_current_refraction.jl:21-39) and the fused refraction tendency. */
+        const int64_t c3 = M->Nx * M->Ny * M->Nk;
+        std::vector<double> U(6 * c3);
+        ora_pm_doppler_velocity(M->Nx, M->Ny, M->Nk, M->Np, N, M->pm_per_cell, M->pm_overlap, nullptr, M->pm_kx,
+                                M->pm_ky, U.data(), U.data() + c3, nullptr, nullptr);
+        ora_current_gradients(M->Nx, M->Ny, M->Nk, U.data(), U.data() + c3, 1.0 / M->dx, 1.0 / M->dy,
+                              U.data() + 2 * c3, U.data() + 3 * c3, U.data() + 4 * c3, U.data() + 5 * c3);
+        ora_model Mc = *M;
+        Mc.Ux = U.data();
+        Mc.Uy = U.data() + c3;
+        Mc.Uxx = U.data() + 2 * c3;
+        Mc.Uxy = U.data() + 3 * c3;
+        Mc.Uyx = U.data() + 4 * c3;
+        Mc.Uyy = U.data() + 5 * c3;
+        refraction_tendency(&Mc, N, G);
+    } else if (M->transport == ORA_TRANSPORT_REFRACTION) refraction_tendency(M, N, G);
     else if (M->transport == ORA_TRANSPORT_INTRINSIC) intrinsic_tendency(M, N, G);
     else std::memset(G, 0, sizeof(double) * total);
     if (with_sources && (M->wind_kind != ORA_WIND_NONE || M->has_dissipation)) add_sources(M, N, t, G);

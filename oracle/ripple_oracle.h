@@ -64,6 +64,13 @@ typedef struct ora_model {
     double beta_max, z_alpha, p_in, alpha0, rho_air, rho_water, von_karman, gravity;
     int32_t has_dissipation;
     double C_ds, B_r, ds_p, sigma_power, ds_gravity;
+    /* PseudomomentumVelocities (current_coupling.jl:41-118): the Doppler velocity is recomputed from the
+     * action before every tendency; Ux..Uyy above are then unused */
+    int32_t pm_mode;
+    int32_t pm_per_cell;                 /* 1: (Nx,Ny,Nk,Nk) overlap tables */
+    const double* pm_overlap;            /* ora_pm_overlap_tables layout */
+    const double* pm_kx;                 /* (Nk,Np) first-moment measures */
+    const double* pm_ky;
 } ora_model;
 
 /* ---- Q kernel (src/Coupling/q_kernel.jl) ---- */
@@ -85,6 +92,19 @@ void ora_doppler_velocity(int64_t Nx, int64_t Ny, int64_t Nz, int64_t Nk,
 void ora_current_gradients(int64_t Nx, int64_t Ny, int64_t Nk,
                            const double* Ux, const double* Uy, double dx_inv, double dy_inv,
                            double* Uxx, double* Uxy, double* Uyx, double* Uyy);
+
+/* ---- pseudomomentum self-coupling (src/Coupling/pseudomomentum.jl) ---- */
+void ora_first_moment_measures(int64_t Nk, int64_t Np, const double* kf, const double* pf, double* kx,
+                               double* ky);
+void ora_pm_overlap_tables(int64_t Nx, int64_t Ny, int64_t Nk, const double* kappa, int64_t Nz,
+                           const double* zf, const double* depth_field, double depth_scalar, double small_mu,
+                           double* overlap, double* doverlap);
+void ora_pm_doppler_velocity(int64_t Nx, int64_t Ny, int64_t Nk, int64_t Np, const double* N, int32_t per_cell,
+                             const double* overlap, const double* doverlap, const double* kx, const double* ky,
+                             double* Ux, double* Uy, double* dUx, double* dUy);
+void ora_pm_cells(int64_t Nx, int64_t Ny, int64_t Nk, int64_t Np, const double* N, int64_t Nz, const double* zf,
+                  const double* depth_field, double depth_scalar, const double* kappa, const double* kx,
+                  const double* ky, double small_mu, int32_t cell_average, double* px, double* py);
 
 /* ---- spectral grid and group velocity ---- */
 void ora_lower_bounded_faces(int64_t N, const double* centers, double lower, double* faces);

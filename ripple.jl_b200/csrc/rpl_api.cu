@@ -70,6 +70,7 @@ cudaError_t dalloc(Handle* h, T** p, size_t count) {
 
 void free_all(Handle* h) {
     rpl::free_learned(h);
+    rpl::free_pm(h);
     void* ptrs[] = {h->N, h->A, h->B, h->d_kappa, h->d_phi, h->d_cos, h->d_sin, h->d_weights, h->d_cgx,
                     h->d_cgy, h->d_cgmag, h->d_depth, h->d_coupling, h->d_wind, h->d_diag, h->d_err,
                     h->d_coef, h->d_tab32, h->d_cell32, h->d_bin32};
@@ -114,6 +115,7 @@ int launch_step(Handle* h, double dt, int stage_only) {
             if (h->learned) RPL_CUDA(rpl::launch_learned_stage_prep(*h, Nin, s));
             else if (h->src.stress_cap) RPL_CUDA(rpl::launch_stress_factor(*h, Nin, s));
         }
+        if (h->pm) RPL_CUDA(rpl::launch_pm_refresh(*h, Nin, s));
         const rpl::StageParams p = rpl::make_params(*h, dt, stage);
         RPL_CUDA(rpl::launch_stage(*h, p, Nin, h->N, Nout, s));
     }
@@ -380,6 +382,8 @@ int rpl_set_currents(rpl_handle* hh, int64_t Nz, const double* z_faces, int32_t 
     }
     const int64_t c3 = P * d.Nk;
     cudaStream_t s = h->stream;
+    RPL_CUDA(cudaStreamSynchronize(s));
+    rpl::free_pm(h);  // prescribed currents replace a pseudomomentum coupling
     if (!h->d_coupling) {
         RPL_CUDA(dalloc(h, &h->d_coupling, 8 * c3));
     }
@@ -418,6 +422,7 @@ int rpl_get_coupling(rpl_handle* hh, double* Ux, double* Uy, double* dUxdk, doub
     Handle* h = reinterpret_cast<Handle*>(hh);
     if (!h->currents_set) return fail(RPL_ERR_STATE, "no currents set");
     const int64_t c3 = h->desc.Nx * h->desc.Ny * h->desc.Nk;
+    if (h->pm) RPL_CUDA(rpl::launch_pm_export(*h, h->stream));
     double* outs[8] = {Ux, Uy, dUxdk, dUydk, Uxx, Uxy, Uyx, Uyy};
     for (int k = 0; k < 8; ++k)
         if (outs[k])
@@ -706,6 +711,7 @@ int rpl_tendency(rpl_handle* hh, double* G, int32_t layout) {
         e = rpl::launch_wind(*h, h->time, s);
         if (e == cudaSuccess && h->src.stress_cap) e = rpl::launch_stress_factor(*h, h->N, s);
     }
+    if (e == cudaSuccess && h->pm) e = rpl::launch_pm_refresh(*h, h->N, s);
     if (e == cudaSuccess) e = rpl::launch_tendency(*h, rpl::make_params(*h, 1.0, 1), h->N, dG, s);
     if (e == cudaSuccess)
         e = rpl::launch_from_device_layout(*h, dG, RPL_F64, dGx, RPL_F64, 0, h->desc.Np, 0, h->desc.Nk, s);

@@ -15,6 +15,51 @@ namespace rpl {
 // switch the scheme to nearly linear weights wherever beta < 1e-3).
 #define RPL_WENO_EPS (10000.0 * DBL_EPSILON)
 
+// ---------------------------------------------------------------- Q kernel (FP64)
+// CDF of the vertical kernel Q (q_kernel.jl:77-85): F(z) = (e^{2mu(s-1)} - e^{-2mu(s+1)}) /
+// (1 - e^{-4mu}), s = clamp((z+d)/d, 0, 1), mu = kappa*d; F = s when |mu| < small_mu.
+// exact_form = 1 evaluates the exponents as the reference does (2mu*s - 2mu); exact_form = 0
+// evaluates them as 2*kappa*z_c and -2*kappa*(z_c + 2d) with z_c = clamp(z, -d, 0), which avoids
+// the cancellation of 2mu*s - 2mu when kappa*d is large.
+__device__ __forceinline__ double q_cdf(double kappa, double z, double d, double small_mu, int exact_form) {
+    const double mu = kappa * d;
+    const double sgn = mu < 0.0 ? -1.0 : 1.0;
+    const double m = fabs(mu) < small_mu ? sgn * small_mu : mu;
+    double s = (z + d) / d;
+    s = s < 0.0 ? 0.0 : (s > 1.0 ? 1.0 : s);
+    double e1, e2;
+    if (exact_form) {
+        const double a = 2.0 * m * s, b = 2.0 * m;
+        e1 = a - b;
+        e2 = -a - b;
+    } else {
+        const double kq = m / d;  // kappa, or the safe-mu kappa
+        double zc = z < -d ? -d : (z > 0.0 ? 0.0 : z);
+        e1 = 2.0 * kq * zc;
+        e2 = -2.0 * kq * (zc + 2.0 * d);
+    }
+    const double fd = (exp(e1) - exp(e2)) / (1.0 - exp(-4.0 * m));
+    return fabs(mu) < small_mu ? s : fd;
+}
+
+// d F / d kappa (q_kernel.jl:94-109).
+__device__ __forceinline__ double q_cdf_dk(double kappa, double z, double d, double small_mu) {
+    const double mu = kappa * d;
+    const double sgn = mu < 0.0 ? -1.0 : 1.0;
+    const double m = fabs(mu) < small_mu ? sgn * small_mu : mu;
+    double s = (z + d) / d;
+    s = s < 0.0 ? 0.0 : (s > 1.0 ? 1.0 : s);
+    const double small_val = d * (4.0 * mu * s * (s * s - 1.0) / 3.0);
+    const double a = exp(-2.0 * m * (1.0 - s));
+    const double b = exp(-2.0 * m * (1.0 + s));
+    const double e = exp(-4.0 * m);
+    const double num = a - b, den = 1.0 - e;
+    const double dnum = -2.0 * (1.0 - s) * a + 2.0 * (1.0 + s) * b;
+    const double dden = 4.0 * e;
+    const double fd = d * (dnum * den - num * dden) / (den * den);
+    return fabs(mu) < small_mu ? small_val : fd;
+}
+
 template <typename T> __device__ __forceinline__ T relu(T x) {
     // max(0, x) with NaN propagation (Julia semantics), -0 -> +0.
     return (x != x) ? x : (x > T(0) ? x : T(0));

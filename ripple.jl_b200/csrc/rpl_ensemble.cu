@@ -341,6 +341,8 @@ int rpl_ensemble_create(rpl_handle* const* members, const double* dt, int32_t co
         if (h.has_sources) return efail(RPL_ERR_UNSUPPORTED, who + "ensemble members carry no sources");
         if (h.desc.transport == RPL_TRANSPORT_REFRACTION && !h.currents_set)
             return efail(RPL_ERR_STATE, who + "refraction transport needs rpl_set_currents first");
+        if (h.pm)
+            return efail(RPL_ERR_UNSUPPORTED, who + "ensemble members take prescribed currents, not pseudomomentum");
     }
     cudaError_t err = cudaSetDevice(h0.device);
     if (err != cudaSuccess) return ecuda(err, "cudaSetDevice");

@@ -131,6 +131,13 @@ struct Handle {
     int64_t lrows = 0;
     bool lclamp = false;           // clamp the network outputs to the output bounds
     bool currents_set = false;
+    // PseudomomentumVelocities (rpl_pm.cu)
+    bool pm = false;               // the coupling is recomputed from the action before every stage
+    bool pm_ready = false;         // d_pmU holds the velocity of some action
+    int64_t pm_cols = 0;           // overlap table pairs: 1 (constant projection depth) or Nx*Ny
+    double* d_pm_overlap = nullptr;  // overlap then derivative overlap, pm_cols x Nk x Nk each
+    double* d_pm_moments = nullptr;  // kx then ky first-moment measures, (Nk, Np) m fastest
+    double* d_pmU = nullptr;         // Ux, Uy, dUx/dkappa, dUy/dkappa, (Nx*Ny*Nk) each, device order
     // sources
     rpl_sources src{};
     bool has_sources = false;
@@ -152,6 +159,12 @@ int mlp_nbins(const rpl_mlp* m);
 const rpl_mlp_desc& mlp_desc(const rpl_mlp* m);
 cudaError_t launch_learned_stage_prep(const Handle& h, const void* Nin, cudaStream_t s);
 void free_learned(Handle* h);
+
+// Pseudomomentum self-coupling (rpl_pm.cu): refresh the velocity and coefficient records from the
+// action Nin; write the caller-order coupling arrays and their gradients into d_coupling; release.
+cudaError_t launch_pm_refresh(Handle& h, const void* Nin, cudaStream_t s);
+cudaError_t launch_pm_export(const Handle& h, cudaStream_t s);
+void free_pm(Handle* h);
 
 // Sets the thread-local message rpl_last_error() returns (rpl_api.cu).
 void set_last_error(const std::string& msg);

@@ -9,8 +9,8 @@ from .grids import (Bounded, Flat, InfiniteDepth, Periodic, PolarWaveVectorGrid,
                     centers_to_faces, lower_bounded_centers_to_faces)
 from .sources import (BulkWindDrag, Clockwise, Counterclockwise, HollandHurricaneWind, LinearStormTrack,
                       LocalSaturationDissipation, PrecomputedSources, PressureCorrelationInput)
-from .model import (Clock, ProductField, Simulation, SpectralWaveModel, WENO, WaveActionField,
-                    compute_tendencies, interior, run_, set_, time_step)
+from .model import (Clock, ProductField, PseudomomentumVelocities, Simulation, SpectralWaveModel, WENO, WaveActionField,
+                    compute_tendencies, interior, run_, set_, time_step, update_coupling)
 from .ensemble import Ensemble
 from . import learned
 from .diagnostics import (diagnostics, m0, mean_direction, mean_period, root_mean_square_wavenumber,

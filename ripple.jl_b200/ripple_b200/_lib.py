@@ -83,6 +83,8 @@ _SIGNATURES = {
     "rpl_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "rpl_set_currents": (ctypes.c_int, [ctypes.c_void_p, _i64, _dp, _i32, _d, _dp, _dp, _dp, _d]),
     "rpl_get_coupling": (ctypes.c_int, [ctypes.c_void_p] + [_dp] * 8),
+    "rpl_set_pseudomomentum": (ctypes.c_int, [ctypes.c_void_p, _i64, _dp, _i32, _d, _dp, _d]),
+    "rpl_update_coupling": (ctypes.c_int, [ctypes.c_void_p]),
     "rpl_set_sources": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(RplSources)]),
     "rpl_set_wind_field": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp]),
     "rpl_set_action": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, _i32, _i32]),

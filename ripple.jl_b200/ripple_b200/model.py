@@ -37,6 +37,25 @@ class Clock:
 _UNSET = object()
 
 
+class PseudomomentumVelocities:
+    """uᴸ = p: the waves' own pseudomomentum drives their Doppler shift (lagrangian_velocities.jl:55-81).
+    The coupling is recomputed from the action before every RK3 stage. Without `q_grid` a Flat wave grid
+    needs a finite model depth; the Q grid is then the stretched automatic grid (Nz, surface_spacing,
+    vertical_stretching as in automatic_q_grid)."""
+
+    def __init__(self, *, q_grid=None, vertical_grid=None, depth=None, Nz=None, surface_spacing=None,
+                 vertical_stretching=2):
+        if depth is not None:
+            raise ArgumentError("`depth` is a SpectralWaveModel kwarg; pass `SpectralWaveModel(...; depth=...)` "
+                                "instead of putting `depth` in `velocities`")
+        if q_grid is not None and vertical_grid is not None:
+            raise ArgumentError("PseudomomentumVelocities cannot contain both `q_grid` and `vertical_grid`")
+        self.q_grid = q_grid if q_grid is not None else vertical_grid
+        self.Nz = Nz
+        self.surface_spacing = surface_spacing
+        self.vertical_stretching = vertical_stretching
+
+
 class ProductField:
     """4-D field N[i, j, m, n] over (x, y) x (kappa, phi) (product_field.jl:29-34).
 
@@ -140,7 +159,7 @@ def _xfast(a):
 
 
 def _automatic_q_grid(grid, cgrid, depth_values, Nz=None, surface_spacing=None, vertical_stretching=2):
-    """Stretched Q-transform grid for Flat wave grids (lagrangian_velocities.jl:344-373)."""
+    """Stretched Q-transform grid for Flat wave grids (lagrangian_velocities.jl:196-225)."""
     H = float(np.max(depth_values))
     kmax = float(np.max(cgrid.κ))
     dz_surface = 1.0 / (20.0 * kmax) if surface_spacing is None else float(surface_spacing)
@@ -204,7 +223,7 @@ class SpectralWaveModel:
         Nx, Ny = grid.Nx, grid.Ny
         Nk, Np = spectral_grid.coordinate_size()
 
-        # depth (lagrangian_velocities.jl:262-335)
+        # depth (lagrangian_velocities.jl:114-187)
         if isinstance(self.depth, InfiniteDepth):
             depth_kind, depth_const, depth_field = _lib.RPL_DEPTH_INFINITE, 0.0, None
         elif isinstance(self.depth, numbers.Number):
@@ -278,8 +297,49 @@ class SpectralWaveModel:
             self._set_action(action.interior())
 
     # ------------------------------------------------------------------ coupling
+    def _q_depth(self, q_grid):
+        """Projection depth of the Q transform: the Q grid's depth for InfiniteDepth, else the model depth
+        (lagrangian_velocities.jl:192-194)."""
+        if isinstance(self.depth, InfiniteDepth):
+            return _lib.RPL_DEPTH_CONSTANT, q_grid.Lz, None
+        if self._depth_field is not None:
+            return _lib.RPL_DEPTH_FIELD, 0.0, self._depth_field
+        return _lib.RPL_DEPTH_CONSTANT, self._depth_const, None
+
+    def _set_pseudomomentum(self, pm):
+        """build_coupling(::PseudomomentumVelocities) (lagrangian_velocities.jl:294-311)."""
+        grid = self.grid
+        q_grid = pm.q_grid
+        if q_grid is None:
+            if grid.has_flat_vertical():
+                if isinstance(self.depth, InfiniteDepth):
+                    raise ArgumentError("Flat wave grids require finite model `depth` or `q_grid` for "
+                                        "PseudomomentumVelocities")
+                dv = self._depth_field if self._depth_field is not None else np.array([self._depth_const])
+                q_grid = _automatic_q_grid(grid, self.spectral_grid, dv, Nz=pm.Nz,
+                                           surface_spacing=pm.surface_spacing,
+                                           vertical_stretching=pm.vertical_stretching)
+            else:
+                q_grid = grid
+        if q_grid.Nx != grid.Nx or q_grid.Ny != grid.Ny or q_grid.has_flat_vertical():
+            raise ArgumentError("velocity `q_grid` must match the wave model grid horizontally and resolve z")
+        qkind, qconst, qfield = self._q_depth(q_grid)
+        self.q_grid = q_grid
+        zf = np.ascontiguousarray(q_grid.zfaces())
+        check(self._lib.rpl_set_pseudomomentum(self._h, q_grid.Nz, dptr(zf), qkind, qconst, dptr(qfield), 1e-6))
+        self._q = dict(zfaces=zf, kind=qkind, const=qconst, field=qfield)
+
+    def update_coupling(self):
+        """update_coupling!(model) (current_coupling.jl:140-148): recompute a pseudomomentum coupling from
+        the current action (prescribed currents are static)."""
+        check(self._lib.rpl_update_coupling(self._h))
+        return self
+
     def _set_velocities(self, velocities):
         grid = self.grid
+        if isinstance(velocities, PseudomomentumVelocities):
+            self._set_pseudomomentum(velocities)
+            return
         if isinstance(velocities, dict):
             u, v = velocities["u"], velocities["v"]
             q_grid = velocities.get("q_grid", velocities.get("vertical_grid"))
@@ -306,13 +366,7 @@ class SpectralWaveModel:
         vv = np.broadcast_to(np.asarray(v(X, Y, Z), dtype=np.float64), X.shape) if callable(v) else np.asarray(v, np.float64)
         if uu.shape != (grid.Nx, grid.Ny, Nz) or vv.shape != uu.shape:
             raise ArgumentError(f"u and v must have size {(grid.Nx, grid.Ny, Nz)}")
-        # Q depth: grid depth for InfiniteDepth (lagrangian_velocities.jl:340-342)
-        if isinstance(self.depth, InfiniteDepth):
-            qkind, qconst, qfield = _lib.RPL_DEPTH_CONSTANT, q_grid.Lz, None
-        elif self._depth_field is not None:
-            qkind, qconst, qfield = _lib.RPL_DEPTH_FIELD, 0.0, self._depth_field
-        else:
-            qkind, qconst, qfield = _lib.RPL_DEPTH_CONSTANT, self._depth_const, None
+        qkind, qconst, qfield = self._q_depth(q_grid)
         self.q_grid = q_grid
         zf = np.ascontiguousarray(q_grid.zfaces())
         self._u, self._v = _xfast(uu), _xfast(vv)
@@ -457,6 +511,11 @@ def time_step(model, dt, nsteps=1):
         model._sync_clock()
     model.clock.last_Δt = dt
     return model
+
+
+def update_coupling(model):
+    """update_coupling!(model) (current_coupling.jl:140-148)."""
+    return model.update_coupling()
 
 
 def compute_tendencies(model):

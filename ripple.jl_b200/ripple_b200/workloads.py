@@ -8,6 +8,8 @@ seamount_eddies    -- 1024^2 x 32 levels at 5 km, periodic; depth 4000 m minus t
                       seamounts (heights 3000-3900 m, widths 50-150 km, clamped >= 100 m); 32 log-spaced
                       kappa in 0.002-0.5 x 36 directions; current = 8 seeded Gaussian eddies (peak
                       0.5 m/s, radius 30-120 km, random sign) times exp(z/200); JONSWAP-like N0; 200 steps.
+self_coupled_swell -- PseudomomentumVelocities: a swell packet Doppler-shifted by its own pseudomomentum
+                      (Flat periodic grid, finite depth, automatic Q grid).
 hurricane_swell    -- 768^2 at 10 km, depth 4000 m, 32 log kappa 0.003-0.3 x 36 directions, no current;
                       translating Holland hurricane (Vmax 50, Rmax 30 km, B 1.5) with wind input and
                       local-saturation whitecapping; N0 = 1e-6; 1000 steps.
@@ -175,6 +177,43 @@ def hurricane_swell(N=768, Nk=32, Np=36, nsteps=1000, L=768 * 10000.0, cfl=0.4, 
     return Workload("hurricane_swell", grid, sg, depth, N0, dt, nsteps, sources=sources,
                     notes={"track": "start (Lx/2, 0.2 Ly), +y at 5 m/s", "radius": 500e3,
                            "inflow_angle_deg": 20.0, "dt_rule": f"CFL {cfl}"})
+
+
+def self_coupled_swell(N=64, Nk=16, Np=24, nsteps=200, dx=2000.0, depth=50.0, depth_field=False, amplitude=4e4,
+                       seed=7, cfl=0.4, peak_velocity=0.3):
+    """PseudomomentumVelocities: a swell packet whose own pseudomomentum Doppler-shifts it. Flat periodic
+    N x N grid at dx; 16 log kappa 0.01-0.3 x 24 directions; finite depth (50 m, or with depth_field a
+    seeded 30-80 m bathymetry) so the Q grid is the automatic stretched one; N0 = amplitude x Gaussian
+    packet (width L/6) x exp(-(ln(kappa/0.05)/0.3)^2) cos^20((phi-0.5)/2) plus a 1e-3 floor. The default
+    amplitude gives a peak Doppler velocity near peak_velocity m/s, which sizes dt with the CFL sum."""
+    from .model import PseudomomentumVelocities
+    L = N * dx
+    grid = RectilinearGrid(size=(N, N), x=(0.0, L), y=(0.0, L), topology=("Periodic", "Periodic", "Flat"))
+    kappa = np.geomspace(0.01, 0.3, Nk)
+    phi = np.arange(Np) * (2.0 * math.pi / Np)
+    sg = PolarWaveVectorGrid(κ=kappa, φ=phi)
+    X, Y = np.meshgrid(grid.xnodes(), grid.ynodes(), indexing="ij")
+    if depth_field:
+        rng = np.random.default_rng(seed)
+        d = np.full((N, N), 80.0)
+        for _ in range(3):
+            cx, cy, w = rng.uniform(0, L), rng.uniform(0, L), rng.uniform(L / 10, L / 4)
+            dX, dY = _periodic_delta(X, cx, L), _periodic_delta(Y, cy, L)
+            d -= rng.uniform(10.0, 25.0) * np.exp(-(dX ** 2 + dY ** 2) / (2 * w ** 2))
+        depth = np.maximum(d, 30.0)
+    K, P = np.meshgrid(kappa, phi, indexing="ij")
+    spec = np.exp(-((np.log(K / 0.05)) / 0.3) ** 2) * np.cos((P - 0.5) / 2) ** 20
+    env = np.exp(-((X - L / 2) ** 2 + (Y - L / 2) ** 2) / (2 * (L / 6) ** 2))
+    N0 = np.asfortranarray(amplitude * env[:, :, None, None] * spec[None, None] + 1e-3)
+    hmax = float(np.max(depth))
+    cg_max = max(0.5 * math.sqrt(G * math.tanh(k * hmax) / k) for k in kappa) + peak_velocity
+    grad = 2.0 * peak_velocity / (L / 6)
+    dk = sg.κ_faces[1] - sg.κ_faces[0]
+    rate = 2 * cg_max / dx + kappa[-1] * 2 * grad / dk + 2 * grad / (2 * math.pi / Np)
+    return Workload("self_coupled_swell", grid, sg, depth, N0, cfl / rate, nsteps,
+                    velocities=PseudomomentumVelocities(),
+                    notes={"amplitude": amplitude, "depth": "field 30-80 m" if depth_field else depth,
+                           "dt_rule": f"CFL sum {cfl}"})
 
 
 ENSEMBLE_SIZES = (64, 128, 256, 384)
