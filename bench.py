@@ -12,6 +12,10 @@ path (the FP64 C++ restatement) on the host cores instead.
 --workload hurricane: 768^2 grid (10 km), 32 kappa x 36 directions, 4000 m depth, moving Holland
 hurricane with Janssen wind input (wave-supported stress cap) and local-saturation whitecapping.
 
+--workload selfcoupled: PseudomomentumVelocities on a 1024^2 grid (2 km, Flat, periodic), 32 kappa x
+36 directions, 50 m depth: a swell packet whose Doppler velocity is recomputed from every stage's
+action (overlap moments + gradients, then the fused refraction stage).
+
 python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--precision fp32|fp64]
                [--workload seamount|hurricane] [--size N]
 Under torchrun each rank advances its own copy of the workload (independent replicas).
@@ -42,7 +46,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
-    ap.add_argument("--workload", default="seamount", choices=["seamount", "hurricane", "ensemble", "learned"])
+    ap.add_argument("--workload", default="seamount", choices=["seamount", "hurricane", "ensemble", "learned",
+                                                                       "selfcoupled"])
     ap.add_argument("--train-steps", type=int, default=40000, help="Adam steps (--workload learned)")
     ap.add_argument("--snapshots", type=int, default=40, help="training snapshots per storm run (--workload learned)")
     ap.add_argument("--dagger", type=int, default=0,
@@ -54,16 +59,23 @@ def parse():
     ap.add_argument("--member-sizes", default="64,128,256,384",
                     help="grid sizes the ensemble members are drawn from (--workload ensemble)")
     ap.add_argument("--size", type=int, default=0, help="grid points per side (default 1024 / 768)")
+    ap.add_argument("--refresh-currents", action="store_true",
+                    help="time-varying currents (--workload seamount): new u, v every step, projected again "
+                         "(rpl_update_currents_device in the timed region; from pinned host buffers in e2e)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
     if args.size <= 0:
-        args.size = 1024 if args.workload in ("seamount", "ensemble") else 768
+        args.size = 1024 if args.workload in ("seamount", "ensemble", "selfcoupled") else 768
     return args
 
 
 WORKLOAD_NAMES = {"seamount": "seamount_eddies", "hurricane": "hurricane_swell", "ensemble": "ensemble_members",
-                  "learned": "hurricane_swell (learned source)"}
+                  "learned": "hurricane_swell (learned source)", "selfcoupled": "self_coupled_swell"}
+TRAFFIC_SUFFIX = {"seamount": "", "hurricane": "_hurricane", "selfcoupled": "_selfcoupled"}
+DATA = {"seamount": "synthetic (seeded seamount depth, eddy currents, JONSWAP-like N0)",
+        "hurricane": "synthetic (Holland hurricane on a linear track, uniform N0 = 1e-6)",
+        "selfcoupled": "synthetic (Gaussian swell packet, 50 m depth, pseudomomentum self-coupling)"}
 
 
 def make_workload(name, n, nsteps, n0_dtype=np.float64):
@@ -74,6 +86,8 @@ def make_workload(name, n, nsteps, n0_dtype=np.float64):
                                          n0_dtype=n0_dtype)
     if name == "seamount":
         return workloads.seamount_eddies(N=n, Nz=32, Nk=32, Np=36, nsteps=nsteps, n0_dtype=n0_dtype)
+    if name == "selfcoupled":
+        return workloads.self_coupled_swell(N=n, Nk=32, Np=36, nsteps=nsteps, n0_dtype=n0_dtype)
     w = workloads.hurricane_swell(N=n, Nk=32, Np=36, nsteps=nsteps)
     if n0_dtype != np.float64:
         w.N0 = w.N0.astype(n0_dtype, order="F")
@@ -81,8 +95,9 @@ def make_workload(name, n, nsteps, n0_dtype=np.float64):
 
 
 def launches_per_step(name):
-    """Our kernels per RK3 step: 3 fused stage kernels; the hurricane adds 1 wind + 3 stress-cap kernels."""
-    return 3 if name == "seamount" else 7
+    """Our kernels per RK3 step: 3 fused stage kernels; the hurricane adds 1 wind + 3 stress-cap kernels;
+    the self-coupled swell adds 2 coupling kernels per stage."""
+    return {"seamount": 3, "selfcoupled": 9}.get(name, 7)
 
 
 def peaks():
@@ -158,6 +173,10 @@ def algorithmic_bytes(w, precision):
     if w.sources is not None:
         cols = w.units // (Nk * Np)
         extra = 3 * (s * w.units + 2 * 32 * cols)
+    if type(w.velocities).__name__ == "PseudomomentumVelocities":
+        # per stage the coupling refresh reads the state once and writes/reads the velocity (32 B) and
+        # rewrites six coefficient fields (48 B) per (i,j,kappa)
+        extra += 3 * (s * w.units + 96 * (w.units // Np))
     return 8 * s * w.units + tables + extra
 
 
@@ -235,20 +254,50 @@ def run_ours(args, rank, world, local_rank):
     _lib.check(lib.rpl_set_stream(h, _lib.ctypes.c_void_p(torch_stream.cuda_stream)))
     dt = w.dt
 
+    # time-varying currents: two current fields (the workload's and a rotated, rescaled copy), device
+    # resident with x fastest, alternated step by step
+    cur = None
+    if args.refresh_currents:
+        if not isinstance(w.velocities, dict):
+            raise SystemExit("--refresh-currents needs a workload with prescribed currents")
+        Nx, Ny, Nz = np.shape(w.velocities["u"])
+        host_cur = []
+        for k in range(2):
+            c, sn, a = math.cos(0.5 * k), math.sin(0.5 * k), 1.0 + 0.2 * k
+            u0, v0 = np.asarray(w.velocities["u"]), np.asarray(w.velocities["v"])
+            pair = []
+            for arr in (a * (c * u0 - sn * v0), a * (sn * u0 + c * v0)):
+                t = torch.empty(arr.size, dtype=torch.float64, pin_memory=True)
+                t.numpy()[:] = np.ravel(arr, order="F")
+                pair.append(t)
+            host_cur.append(pair)
+        cur = [[t.to(f"cuda:{local_rank}") for t in pair] for pair in host_cur]
+        torch.cuda.synchronize()
+
+    def refresh(k):
+        _lib.check(lib.rpl_update_currents_device(h, _lib.ctypes.c_void_p(cur[k % 2][0].data_ptr()),
+                                                  _lib.ctypes.c_void_p(cur[k % 2][1].data_ptr())))
+
     # warm-up
-    for _ in range(args.warmup):
+    for k in range(args.warmup):
+        if cur is not None:
+            refresh(k)
         _lib.check(lib.rpl_step_async(h, dt, 1))
     _lib.check(lib.rpl_sync(h))
     barrier()
 
     # device-timed region: K steps, events around each stage launch on the launching stream
     ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
+    rev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(smi_id) as clk:
         barrier()
         with torch.cuda.stream(torch_stream):
             start.record(torch_stream)
             for k in range(args.steps):
+                if cur is not None:
+                    rev[k].record(torch_stream)
+                    refresh(k)
                 ev[k][0].record(torch_stream)
                 for s in (1, 2, 3):
                     _lib.check(lib.rpl_stage_async(h, dt, s))
@@ -259,6 +308,7 @@ def run_ours(args, rank, world, local_rank):
         barrier()
     ms = start.elapsed_time(end)
     stage_ms = [ev[k][s].elapsed_time(ev[k][s + 1]) for k in range(args.steps) for s in range(3)]
+    refresh_ms = statistics.mean(rev[k].elapsed_time(ev[k][0]) for k in range(args.steps)) if cur else None
     if dist is not None:
         t = torch.tensor([ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -275,7 +325,7 @@ def run_ours(args, rank, world, local_rank):
     tp = os.path.join(ROOT, "profiles", "stage_traffic.json")
     if os.path.exists(tp):
         try:
-            key = f"{args.precision}_{args.size}" + ("" if args.workload == "seamount" else "_hurricane")
+            key = f"{args.precision}_{args.size}" + TRAFFIC_SUFFIX[args.workload]
             traffic = json.load(open(tp)).get(key)
         except Exception:
             traffic = None
@@ -292,7 +342,10 @@ def run_ours(args, rank, world, local_rank):
         t0 = time.perf_counter()
         _lib.check(lib.rpl_set_action(h, _lib.ctypes.c_void_p(host.data_ptr()),
                                       _lib.RPL_F32 if args.precision == "fp32" else _lib.RPL_F64, 0))
-        for _ in range(args.steps):
+        for k in range(args.steps):
+            if cur is not None:
+                _lib.check(lib.rpl_update_currents(h, _lib.dptr(host_cur[k % 2][0].numpy()),
+                                                   _lib.dptr(host_cur[k % 2][1].numpy())))
             _lib.check(lib.rpl_step(h, dt, 1))
             _lib.check(lib.rpl_diagnostics(h, None, None, None, None, _lib.dptr(tot)))
         _lib.check(lib.rpl_get_action(h, _lib.ctypes.c_void_p(host.data_ptr()),
@@ -303,9 +356,12 @@ def run_ours(args, rank, world, local_rank):
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             el = float(t.item())
         nbytes = host.numel() * host.element_size()
+        cur_bytes = 2 * host_cur[0][0].numel() * 8 if cur is not None else 0
         e2e = {"value": world * w.units * args.steps / el, "unit": UNIT,
-               "h2d_bytes_per_step": nbytes / args.steps, "d2h_bytes_per_step": (nbytes + 8 * args.steps) / args.steps,
-               "includes": "set! from pinned host, K x (time_step! + total_action read), interior to pinned host"}
+               "h2d_bytes_per_step": nbytes / args.steps + cur_bytes,
+               "d2h_bytes_per_step": (nbytes + 8 * args.steps) / args.steps,
+               "includes": "set! from pinned host, K x (" + ("new currents from pinned host + " if cur else "") +
+                           "time_step! + total_action read), interior to pinned host"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -316,20 +372,23 @@ def run_ours(args, rank, world, local_rank):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32" if args.precision == "fp32" else "f64",
-            "data": ("synthetic (seeded seamount depth, eddy currents, JONSWAP-like N0)" if args.workload == "seamount"
-                     else "synthetic (Holland hurricane on a linear track, uniform N0 = 1e-6)"),
+            "data": DATA[args.workload],
             "config": {"workload": WORKLOAD_NAMES[args.workload], "grid": [args.size, args.size],
                        "spectral": [32, 36],
                        "precision": args.precision, "units_per_step": w.units, "dt": dt,
                        "l2": "state (%.1f GB per buffer) larger than L2; no flush" % (w.units * (4 if args.precision == "fp32" else 8) / 1e9),
-                       "parallelism": f"{world} independent replicas" if world > 1 else "1 GPU"},
+                       "parallelism": f"{world} independent replicas" if world > 1 else "1 GPU",
+                       **({"currents": "time-varying: new u, v every step (Q transform + gradients + coefficients "
+                                       "in the timed region)", "currents_refresh_ms": refresh_ms} if cur else {})},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "peak_kind": peak_kind,
                          "kernel": "tile_kernel" if args.precision == "fp32" else "column_kernel",
                          "launch_ms": launch_ms, "algorithmic_bytes_per_launch": bytes_per_launch,
-                         "launch_interval": "one RK3 stage" + ("" if args.workload == "seamount"
-                                                               else " incl. its wind/stress-cap kernels")},
-            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches_per_step(args.workload) * args.steps,
+                         "launch_interval": "one RK3 stage" + {"seamount": "",
+                                                               "selfcoupled": " incl. its coupling refresh"}.get(
+                                                                   args.workload, " incl. its wind/stress-cap kernels")},
+            "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": (launches_per_step(args.workload) + (3 if cur else 0)) * args.steps,
             "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
@@ -460,7 +519,9 @@ def run_ensemble(args, rank, world, local_rank):
                        "speedup_vs_sequential": ms_seq / ms,
                        "build_s": t_build, "autotune_s": t_tune,
                        "l2": "state (%.1f GB per buffer set) larger than L2; no flush" % (4 * units / 1e9),
-                       "parallelism": f"{world} independent replicas" if world > 1 else "1 GPU"},
+                       "parallelism": f"{world} independent replicas" if world > 1 else "1 GPU",
+                       **({"currents": "time-varying: new u, v every step (Q transform + gradients + coefficients "
+                                       "in the timed region)", "currents_refresh_ms": refresh_ms} if cur else {})},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": None, "peak_kind": peak_kind, "kernel": "ensemble_kernel",
                          "launch_ms": launch_ms, "algorithmic_bytes_per_launch": nbytes_alg / 3.0,

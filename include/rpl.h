@@ -127,6 +127,16 @@ int rpl_destroy(rpl_handle* h);
 int rpl_set_currents(rpl_handle* h, int64_t Nz, const double* z_faces,
                      int32_t q_depth_kind, double q_depth_constant, const double* q_depth_field,
                      const double* u, const double* v, double small_mu);
+/* Replaces update_coupling!(coupling::CWCMPrescribedCurrentCoupling) after the current fields changed
+ * (current_coupling.jl:127-138): recomputes the Doppler velocity, its gradients and the stage
+ * coefficients from new u, v ((Nx,Ny,Nz) x fastest, host memory) on the Q grid of the last
+ * rpl_set_currents, in stream order and without allocating, so time-varying currents can be refreshed
+ * every step. The copies are stream-ordered: pinned host buffers must stay unchanged until the next
+ * rpl_sync. Values are not scanned on the host; non-finite currents surface as RPL_ERR_DEVICE from the
+ * step that uses them. */
+int rpl_update_currents(rpl_handle* h, const double* u, const double* v);
+/* The same with u, v in device memory on the handle's device (read in stream order, not copied). */
+int rpl_update_currents_device(rpl_handle* h, const double* u, const double* v);
 /* Replaces build_coupling(PseudomomentumVelocities) + CWCMPseudomomentumCoupling
  * (lagrangian_velocities.jl:294-311, current_coupling.jl:93-118): builds the vertical overlap tables of
  * the Q transform (pseudomomentum.jl:68-121; one Nk x Nk pair for RPL_DEPTH_CONSTANT, one per (i,j) for

@@ -195,11 +195,13 @@ class Oracle:
             m.transport = TRANSPORT_NONE
         self._set_sources(w.sources)
 
-    def _set_currents(self, w):
+    def _set_currents(self, w, u=None, v=None):
         L = lib()
         g = w.grid
         q_grid = w.velocities.get("q_grid", g)
-        u, v = xfast(w.velocities["u"]), xfast(w.velocities["v"])
+        if u is None:
+            u, v = w.velocities["u"], w.velocities["v"]
+        u, v = xfast(u), xfast(v)
         zf = f64(q_grid.zfaces())
         Nz = len(zf) - 1
         depth = w.depth
@@ -220,6 +222,11 @@ class Oracle:
                                 p(self.U["Ux_x"]), p(self.U["Ux_y"]), p(self.U["Uy_x"]), p(self.U["Uy_y"]))
         m.Ux, m.Uy = p(self.U["Ux"]), p(self.U["Uy"])
         m.Uxx, m.Uxy, m.Uyx, m.Uyy = p(self.U["Ux_x"]), p(self.U["Ux_y"]), p(self.U["Uy_x"]), p(self.U["Uy_y"])
+
+    def update_currents(self, u, v):
+        """New currents on the same Q grid: update_coupling!(::CWCMPrescribedCurrentCoupling)
+        (current_coupling.jl:127-138)."""
+        self._set_currents(self.w, u, v)
 
     def _q_faces_and_depth(self, w, q_grid, Nz=None, surface_spacing=None, stretch=2.0):
         """Q-transform z faces and projection depth (lagrangian_velocities.jl:192-225,294-311)."""

@@ -71,13 +71,46 @@ cudaError_t dalloc(Handle* h, T** p, size_t count) {
 void free_all(Handle* h) {
     rpl::free_learned(h);
     rpl::free_pm(h);
+    rpl::free_currents(h);
     void* ptrs[] = {h->N, h->A, h->B, h->d_kappa, h->d_phi, h->d_cos, h->d_sin, h->d_weights, h->d_cgx,
                     h->d_cgy, h->d_cgmag, h->d_depth, h->d_coupling, h->d_wind, h->d_diag, h->d_err,
-                    h->d_coef, h->d_tab32, h->d_cell32, h->d_bin32};
+                    h->d_coef, h->d_tab32, h->d_cell32, h->d_bin32, h->d_U};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->h_err) cudaFreeHost(h->h_err);
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+}
+
+}  // namespace
+
+// Releases the prescribed-currents state (Q grid, weight tables, the device copy of u and v).
+void rpl::free_currents(Handle* h) {
+    const int64_t P = h->cells, Nk = h->desc.Nk;
+    if (h->d_qz) h->bytes -= (h->q_Nz + 1) * 8;
+    if (h->d_qdepth) h->bytes -= P * 8;
+    if (h->d_qW) h->bytes -= 2 * h->q_Nz * Nk * 8;
+    if (h->d_cur) h->bytes -= 2 * P * h->q_Nz * 8;
+    if (h->d_qcol) h->bytes -= P * h->q_Nz * Nk * (h->q_col_f32 ? 4 : 8);
+    for (double* p : {h->d_qz, h->d_qdepth, h->d_qW, h->d_cur})
+        if (p) cudaFree(p);
+    if (h->d_qcol) cudaFree(h->d_qcol);
+    h->d_qz = h->d_qdepth = h->d_qW = h->d_cur = nullptr;
+    h->d_qcol = nullptr;
+    h->q_Nz = 0;
+    h->dU_stale = false;
+}
+
+namespace {
+
+// Doppler velocity of the currents (u, v device pointers, (Nx,Ny,Nz) x fastest) on the stored Q grid,
+// then its gradients and the coefficient records, in stream order. The stage kernels do not read
+// dU/dkappa; it is recomputed from d_cur when rpl_get_coupling asks for it.
+cudaError_t refresh_currents(Handle* h, const double* u, const double* v, cudaStream_t s) {
+    const int64_t c3 = h->cells * h->desc.Nk;
+    cudaError_t e = rpl::launch_doppler(*h, u, v, 0, h->d_U, h->d_U + c3, s);
+    if (e == cudaSuccess) e = rpl::launch_coef_from_U(*h, s);
+    if (e == cudaSuccess) h->dU_stale = true;
+    return e;
 }
 
 int check_handle(rpl_handle* hh) {
@@ -381,37 +414,89 @@ int rpl_set_currents(rpl_handle* hh, int64_t Nz, const double* z_faces, int32_t 
         return fail(RPL_ERR_ARGUMENT, "Q-transform depth must be constant or a field");
     }
     const int64_t c3 = P * d.Nk;
+    const bool field = q_depth_kind == RPL_DEPTH_FIELD;
+    const int64_t extra = (h->d_coupling ? 0 : 8 * c3 * 8) + (h->d_U ? 0 : 4 * c3 * 8) + (Nz + 1) * 8 +
+                          (field ? P * 8 : 2 * Nz * d.Nk * 8) + 2 * n3 * 8;
     cudaStream_t s = h->stream;
     RPL_CUDA(cudaStreamSynchronize(s));
     rpl::free_pm(h);  // prescribed currents replace a pseudomomentum coupling
-    if (!h->d_coupling) {
-        RPL_CUDA(dalloc(h, &h->d_coupling, 8 * c3));
+    rpl::free_currents(h);
+    if (d.memory_limit_bytes > 0 && h->bytes + extra > d.memory_limit_bytes)
+        return fail(RPL_ERR_OOM, "currents need " + std::to_string(extra) + " more device bytes, above the memory limit");
+    h->currents_set = false;
+    if (!h->d_coupling) RPL_CUDA(dalloc(h, &h->d_coupling, 8 * c3));
+    if (!h->d_U) RPL_CUDA(dalloc(h, &h->d_U, 4 * c3));
+    cudaError_t e = dalloc(h, &h->d_qz, Nz + 1);
+    if (e == cudaSuccess && field) e = dalloc(h, &h->d_qdepth, P);
+    if (e == cudaSuccess && !field) e = dalloc(h, &h->d_qW, 2 * Nz * d.Nk);
+    if (e == cudaSuccess) e = dalloc(h, &h->d_cur, 2 * n3);
+    if (e != cudaSuccess) {
+        rpl::free_currents(h);
+        cudaGetLastError();
+        return fail(RPL_ERR_OOM, "currents: device allocation failed");
     }
-    double *du = nullptr, *dv = nullptr, *dz = nullptr, *dq = nullptr;
-    cudaError_t e = cudaMalloc(&du, n3 * 8);
-    if (e == cudaSuccess) e = cudaMalloc(&dv, n3 * 8);
-    if (e == cudaSuccess) e = cudaMalloc(&dz, (Nz + 1) * 8);
-    if (e == cudaSuccess && q_depth_kind == RPL_DEPTH_FIELD) e = cudaMalloc(&dq, P * 8);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(du, u, n3 * 8, cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(dv, v, n3 * 8, cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(dz, z_faces, (Nz + 1) * 8, cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess && dq) e = cudaMemcpyAsync(dq, q_depth_field, P * 8, cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess) e = rpl::launch_doppler(*h, Nz, du, dv, dz, dq, q_depth_constant, small_mu, s);
-    if (e == cudaSuccess) e = rpl::launch_gradients(*h, s);
+    h->q_Nz = Nz;
+    h->q_const = field ? 0.0 : q_depth_constant;
+    h->q_small_mu = small_mu;
+    e = cudaMemcpyAsync(h->d_cur, u, n3 * 8, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h->d_cur + n3, v, n3 * 8, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h->d_qz, z_faces, (Nz + 1) * 8, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess && field) e = cudaMemcpyAsync(h->d_qdepth, q_depth_field, P * 8, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess && !field)
+        e = rpl::launch_q_table(*h, Nz, h->d_qz, q_depth_constant, small_mu, h->d_qW, h->d_qW + Nz * d.Nk, s);
+    if (e == cudaSuccess && field) {
+        // per-column Q weights (FP32 for FP32 models): refreshes then stream them instead of evaluating
+        // the Q kernel's exponentials again; skipped when they would exceed the memory limit or fail to
+        // allocate
+        h->q_col_f32 = h->precision == RPL_FP32;
+        const int64_t tb = P * Nz * d.Nk * (h->q_col_f32 ? 4 : 8);
+        if (!(d.memory_limit_bytes > 0 && h->bytes + tb > d.memory_limit_bytes) &&
+            cudaMalloc(&h->d_qcol, tb) == cudaSuccess) {
+            h->bytes += tb;
+            e = rpl::launch_q_column_table(*h, s);
+        } else {
+            cudaGetLastError();
+            h->d_qcol = nullptr;
+        }
+    }
     if (e == cudaSuccess) {
         h->currents_set = true;  // the coefficient records read the coupling from here on
-        e = rpl::launch_coef(*h, s);
+        e = refresh_currents(h, h->d_cur, h->d_cur + n3, s);
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    cudaFree(du);
-    cudaFree(dv);
-    cudaFree(dz);
-    if (dq) cudaFree(dq);
     if (e != cudaSuccess) {
         h->currents_set = false;
+        rpl::free_currents(h);
         return cuda_fail(e, "rpl_set_currents");
     }
-    h->currents_set = true;
+    return RPL_OK;
+}
+
+int rpl_update_currents(rpl_handle* hh, const double* u, const double* v) {
+    int st = check_handle(hh);
+    if (st) return st;
+    Handle* h = reinterpret_cast<Handle*>(hh);
+    if (!u || !v) return fail(RPL_ERR_ARGUMENT, "null u or v");
+    if (!h->d_cur || h->pm) return fail(RPL_ERR_STATE, "rpl_update_currents needs rpl_set_currents first");
+    const int64_t n3 = h->cells * h->q_Nz;
+    cudaStream_t s = h->stream;
+    RPL_CUDA(cudaMemcpyAsync(h->d_cur, u, n3 * 8, cudaMemcpyHostToDevice, s));
+    RPL_CUDA(cudaMemcpyAsync(h->d_cur + n3, v, n3 * 8, cudaMemcpyHostToDevice, s));
+    RPL_CUDA(refresh_currents(h, h->d_cur, h->d_cur + n3, s));
+    return RPL_OK;
+}
+
+int rpl_update_currents_device(rpl_handle* hh, const double* u, const double* v) {
+    int st = check_handle(hh);
+    if (st) return st;
+    Handle* h = reinterpret_cast<Handle*>(hh);
+    if (!u || !v) return fail(RPL_ERR_ARGUMENT, "null u or v");
+    if (!h->d_cur || h->pm) return fail(RPL_ERR_STATE, "rpl_update_currents_device needs rpl_set_currents first");
+    // kept for the dU/dkappa caches that rpl_get_coupling computes on request
+    const int64_t n3 = h->cells * h->q_Nz;
+    RPL_CUDA(cudaMemcpyAsync(h->d_cur, u, n3 * 8, cudaMemcpyDeviceToDevice, h->stream));
+    RPL_CUDA(cudaMemcpyAsync(h->d_cur + n3, v, n3 * 8, cudaMemcpyDeviceToDevice, h->stream));
+    RPL_CUDA(refresh_currents(h, h->d_cur, h->d_cur + n3, h->stream));
     return RPL_OK;
 }
 
@@ -422,7 +507,12 @@ int rpl_get_coupling(rpl_handle* hh, double* Ux, double* Uy, double* dUxdk, doub
     Handle* h = reinterpret_cast<Handle*>(hh);
     if (!h->currents_set) return fail(RPL_ERR_STATE, "no currents set");
     const int64_t c3 = h->desc.Nx * h->desc.Ny * h->desc.Nk;
-    if (h->pm) RPL_CUDA(rpl::launch_pm_export(*h, h->stream));
+    if (!h->pm && h->dU_stale) {
+        const int64_t n3 = h->cells * h->q_Nz;
+        RPL_CUDA(rpl::launch_doppler(*h, h->d_cur, h->d_cur + n3, 1, h->d_U + 2 * c3, h->d_U + 3 * c3, h->stream));
+        h->dU_stale = false;
+    }
+    RPL_CUDA(rpl::launch_export_U(*h, h->stream));
     double* outs[8] = {Ux, Uy, dUxdk, dUydk, Uxx, Uxy, Uyx, Uyy};
     for (int k = 0; k < 8; ++k)
         if (outs[k])

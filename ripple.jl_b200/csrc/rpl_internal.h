@@ -116,7 +116,10 @@ struct Handle {
     double* d_cgy = nullptr;
     double* d_cgmag = nullptr;
     double* d_depth = nullptr;
-    double* d_coupling = nullptr;  // 8 arrays of (Nx,Ny,Nk): Ux Uy dUxdk dUydk Uxx Uxy Uyx Uyy
+    double* d_coupling = nullptr;  // 8 arrays of (Nx,Ny,Nk): Ux Uy dUxdk dUydk Uxx Uxy Uyx Uyy (caller order,
+                                   // filled from d_U when rpl_get_coupling asks)
+    double* d_U = nullptr;         // Doppler velocity in device order c*Nk + m: Ux, Uy, dUx/dkappa,
+                                   // dUy/dkappa, (Nx*Ny*Nk) each (prescribed or pseudomomentum)
     double* d_coef = nullptr;      // (Nx*Ny*Nk) records of 8 doubles in device order
     float* d_tab32 = nullptr;      // FP32 copies: 4*Np trig, 2*Nk*Np group velocity, 2*Np cos/sin, Nk*Np weights
     float* d_cell32 = nullptr;     // (Nx*Ny) x 8 floats of per-cell wind constants
@@ -131,13 +134,23 @@ struct Handle {
     int64_t lrows = 0;
     bool lclamp = false;           // clamp the network outputs to the output bounds
     bool currents_set = false;
+    // prescribed currents: the Q grid and the last currents stay on the device so the coupling can be
+    // refreshed (rpl_update_currents*) without allocating
+    int64_t q_Nz = 0;
+    double q_const = 0.0, q_small_mu = 0.0;
+    double* d_qz = nullptr;        // Nz+1 z faces
+    double* d_qdepth = nullptr;    // (Nx,Ny) projection depth, depth fields only
+    double* d_qW = nullptr;        // constant depth: Q cell weights W then Wd, (Nz, Nk) each, m fastest
+    double* d_cur = nullptr;       // u then v, (Nx,Ny,Nz) each, x fastest
+    void* d_qcol = nullptr;        // depth field: per-column Q weights (Nz, Nk) per column, when memory allows
+    bool q_col_f32 = false;        // d_qcol holds floats (FP32 models)
+    bool dU_stale = false;         // the dU/dkappa caches lag the last currents (computed on request)
     // PseudomomentumVelocities (rpl_pm.cu)
     bool pm = false;               // the coupling is recomputed from the action before every stage
-    bool pm_ready = false;         // d_pmU holds the velocity of some action
+    bool pm_ready = false;         // d_U holds the velocity of some action
     int64_t pm_cols = 0;           // overlap table pairs: 1 (constant projection depth) or Nx*Ny
     double* d_pm_overlap = nullptr;  // overlap then derivative overlap, pm_cols x Nk x Nk each
     double* d_pm_moments = nullptr;  // kx then ky first-moment measures, (Nk, Np) m fastest
-    double* d_pmU = nullptr;         // Ux, Uy, dUx/dkappa, dUy/dkappa, (Nx*Ny*Nk) each, device order
     // sources
     rpl_sources src{};
     bool has_sources = false;
@@ -163,16 +176,22 @@ void free_learned(Handle* h);
 // Pseudomomentum self-coupling (rpl_pm.cu): refresh the velocity and coefficient records from the
 // action Nin; write the caller-order coupling arrays and their gradients into d_coupling; release.
 cudaError_t launch_pm_refresh(Handle& h, const void* Nin, cudaStream_t s);
-cudaError_t launch_pm_export(const Handle& h, cudaStream_t s);
 void free_pm(Handle* h);
+// Releases the prescribed-currents state of rpl_set_currents (rpl_api.cu).
+void free_currents(Handle* h);
 
 // Sets the thread-local message rpl_last_error() returns (rpl_api.cu).
 void set_last_error(const std::string& msg);
 
 // ---- launchers (rpl_setup.cu) ----
-cudaError_t launch_doppler(const Handle& h, int64_t Nz, const double* d_u, const double* d_v,
-                           const double* d_zf, const double* d_qdepth, double qdepth_const,
-                           double small_mu, cudaStream_t s);
+cudaError_t launch_q_table(const Handle& h, int64_t Nz, const double* d_zf, double qdepth_const, double small_mu,
+                           double* W, double* Wd, cudaStream_t s);
+// Per-column Q weights of a depth field into h.d_qcol (FP32 when h.q_col_f32).
+cudaError_t launch_q_column_table(const Handle& h, cudaStream_t s);
+// Doppler velocity (derivative = 0) or its kappa derivative (1) of the currents d_u, d_v on the Q grid
+// of rpl_set_currents, into the caller-order arrays Ux, Uy.
+cudaError_t launch_doppler(const Handle& h, const double* d_u, const double* d_v, int derivative, double* Ux,
+                           double* Uy, cudaStream_t s);
 cudaError_t launch_gradients(const Handle& h, cudaStream_t s);
 cudaError_t launch_cg_field(const Handle& h, cudaStream_t s);
 cudaError_t launch_wind(const Handle& h, double t, cudaStream_t s);
@@ -186,6 +205,10 @@ cudaError_t launch_to_device_layout(const Handle& h, const void* src, int src_dt
 cudaError_t launch_from_device_layout(const Handle& h, const void* src, int src_dtype, void* dst, int dst_dtype,
                                       int64_t n0, int64_t nc, int64_t m0, int64_t mc, cudaStream_t s);
 cudaError_t launch_coef(const Handle& h, cudaStream_t s);
+// Coefficient fields 0-5 (Ux, Uy and the periodic gradients) from the device-order velocity d_U.
+cudaError_t launch_coef_from_U(const Handle& h, cudaStream_t s);
+// d_U -> the caller-order coupling arrays 0-3 of d_coupling, then their gradients (arrays 4-7).
+cudaError_t launch_export_U(const Handle& h, cudaStream_t s);
 
 // ---- FP32 tiled stage kernel (rpl_tile32.cu) ----
 bool tile32_supported(const Handle& h);

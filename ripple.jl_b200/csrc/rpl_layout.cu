@@ -80,6 +80,40 @@ __global__ void coef_kernel(int64_t Nx, int64_t Ny, int64_t Nk, const double* __
     r[7] = kappa[m];
 }
 
+// Coefficient records (Ux, Uy, Ux_x, Ux_y, Uy_x, Uy_y; fields 6 and 7 stay) from the device-order
+// velocity, with the periodic centred gradients of wave_current_refraction.jl:7-19.
+__global__ void coef_from_U_kernel(int64_t Nx, int64_t Ny, int Nk, const double* __restrict__ U, double dx_inv,
+                               double dy_inv, double* __restrict__ coef) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t P = Nx * Ny, c3 = P * Nk;
+    if (t >= c3) return;
+    const int64_t c = t / Nk, m = t - c * Nk;
+    const int64_t j = c / Nx, i = c - j * Nx;
+    const int64_t ip = i == Nx - 1 ? 0 : i + 1, im = i == 0 ? Nx - 1 : i - 1;
+    const int64_t jp = j == Ny - 1 ? 0 : j + 1, jm = j == 0 ? Ny - 1 : j - 1;
+    const int64_t xp = (j * Nx + ip) * Nk + m, xm = (j * Nx + im) * Nk + m;
+    const int64_t yp = (jp * Nx + i) * Nk + m, ym = (jm * Nx + i) * Nk + m;
+    const double* Uy = U + c3;
+    double* r = coef + 8 * t;
+    r[0] = U[t];
+    r[1] = Uy[t];
+    r[2] = (U[xp] - U[xm]) * (dx_inv / 2.0);
+    r[3] = (U[yp] - U[ym]) * (dy_inv / 2.0);
+    r[4] = (Uy[xp] - Uy[xm]) * (dx_inv / 2.0);
+    r[5] = (Uy[yp] - Uy[ym]) * (dy_inv / 2.0);
+}
+
+// Device-order velocity -> the caller-order coupling arrays Ux, Uy, dUx/dkappa, dUy/dkappa (x fastest).
+__global__ void export_U_kernel(int64_t P, int Nk, const double* __restrict__ U, double* __restrict__ out) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t c3 = P * Nk;
+    if (t >= c3) return;
+    const int64_t c = t / Nk, m = t - c * Nk;
+    const int64_t x = c + P * m;
+#pragma unroll
+    for (int a = 0; a < 4; ++a) out[a * c3 + x] = U[a * c3 + t];
+}
+
 template <typename S, typename D>
 cudaError_t to_dev(const void* src, void* dst, const Handle& h, int64_t n0, int64_t nc, int64_t m0, int64_t mc,
                    cudaStream_t s) {
@@ -122,6 +156,22 @@ cudaError_t launch_coef(const Handle& h, cudaStream_t s) {
     coef_kernel<<<(unsigned)((c3 + 255) / 256), 256, 0, s>>>(d.Nx, d.Ny, d.Nk, h.currents_set ? h.d_coupling : nullptr,
                                                              h.d_cgmag, h.d_kappa, h.d_coef);
     return cudaGetLastError();
+}
+
+cudaError_t launch_coef_from_U(const Handle& h, cudaStream_t s) {
+    const rpl_desc& d = h.desc;
+    const int64_t c3 = d.Nx * d.Ny * d.Nk;
+    coef_from_U_kernel<<<(unsigned)((c3 + 255) / 256), 256, 0, s>>>(d.Nx, d.Ny, (int)d.Nk, h.d_U, 1.0 / d.dx,
+                                                                    1.0 / d.dy, h.d_coef);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_export_U(const Handle& h, cudaStream_t s) {
+    const int64_t c3 = h.cells * h.desc.Nk;
+    export_U_kernel<<<(unsigned)((c3 + 255) / 256), 256, 0, s>>>(h.cells, (int)h.desc.Nk, h.d_U, h.d_coupling);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return launch_gradients(h, s);
 }
 
 }  // namespace rpl

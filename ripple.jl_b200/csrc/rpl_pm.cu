@@ -9,8 +9,9 @@
 //                       for every source ring s (lanes over s, coalesced kappa-contiguous reads of the
 //                       state), then U_t = sum_s overlap[t,s] M_s and dU/dkappa_t with the derivative
 //                       table (lanes over targets t); written kappa-fastest per column.
-//   pm_coef_kernel      the periodic centred gradients of Ux, Uy (wave_current_refraction.jl:7-19)
-//                       fused with the write of the stage kernels' coefficient records.
+//   coef_from_U_kernel  (rpl_layout.cu) the periodic centred gradients of Ux, Uy
+//                       (wave_current_refraction.jl:7-19) fused with the write of the stage kernels'
+//                       coefficient records.
 // The caller-order coupling arrays (rpl_get_coupling) are produced on request only.
 #include <cuda_runtime.h>
 
@@ -127,40 +128,6 @@ pm_velocity_kernel(const T* __restrict__ N, int64_t P, int Nk, int Np, const dou
     }
 }
 
-// Coefficient records (Ux, Uy, Ux_x, Ux_y, Uy_x, Uy_y; fields 6 and 7 stay) from the device-order
-// velocity, with the periodic centred gradients of wave_current_refraction.jl:7-19.
-__global__ void pm_coef_kernel(int64_t Nx, int64_t Ny, int Nk, const double* __restrict__ U, double dx_inv,
-                               double dy_inv, double* __restrict__ coef) {
-    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int64_t P = Nx * Ny, c3 = P * Nk;
-    if (t >= c3) return;
-    const int64_t c = t / Nk, m = t - c * Nk;
-    const int64_t j = c / Nx, i = c - j * Nx;
-    const int64_t ip = i == Nx - 1 ? 0 : i + 1, im = i == 0 ? Nx - 1 : i - 1;
-    const int64_t jp = j == Ny - 1 ? 0 : j + 1, jm = j == 0 ? Ny - 1 : j - 1;
-    const int64_t xp = (j * Nx + ip) * Nk + m, xm = (j * Nx + im) * Nk + m;
-    const int64_t yp = (jp * Nx + i) * Nk + m, ym = (jm * Nx + i) * Nk + m;
-    const double* Uy = U + c3;
-    double* r = coef + 8 * t;
-    r[0] = U[t];
-    r[1] = Uy[t];
-    r[2] = (U[xp] - U[xm]) * (dx_inv / 2.0);
-    r[3] = (U[yp] - U[ym]) * (dy_inv / 2.0);
-    r[4] = (Uy[xp] - Uy[xm]) * (dx_inv / 2.0);
-    r[5] = (Uy[yp] - Uy[ym]) * (dy_inv / 2.0);
-}
-
-// Device-order velocity -> the caller-order coupling arrays Ux, Uy, dUx/dkappa, dUy/dkappa (x fastest).
-__global__ void pm_export_kernel(int64_t P, int Nk, const double* __restrict__ U, double* __restrict__ out) {
-    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int64_t c3 = P * Nk;
-    if (t >= c3) return;
-    const int64_t c = t / Nk, m = t - c * Nk;
-    const int64_t x = c + P * m;
-#pragma unroll
-    for (int a = 0; a < 4; ++a) out[a * c3 + x] = U[a * c3 + t];
-}
-
 inline unsigned blocks_for(int64_t n, int threads) { return (unsigned)((n + threads - 1) / threads); }
 
 int overlap_chunk(int Nk) { return std::max(1, std::min(32, 2048 / Nk)); }
@@ -170,7 +137,7 @@ int overlap_chunk(int Nk) { return std::max(1, std::min(32, 2048 / Nk)); }
 cudaError_t launch_pm_refresh(Handle& h, const void* Nin, cudaStream_t s) {
     const rpl_desc& d = h.desc;
     const int Nk = (int)d.Nk, Np = (int)d.Np;
-    const int64_t P = h.cells, c3 = P * Nk;
+    const int64_t P = h.cells;
     const size_t smem = (size_t)PM_WARPS * 2 * Nk * sizeof(double);
     const unsigned blocks = blocks_for(P, PM_WARPS);
     const double* O = h.d_pm_overlap;
@@ -178,36 +145,25 @@ cudaError_t launch_pm_refresh(Handle& h, const void* Nin, cudaStream_t s) {
     if (h.precision == RPL_FP64)
         pm_velocity_kernel<double><<<blocks, PM_WARPS * 32, smem, s>>>((const double*)Nin, P, Nk, Np, h.d_pm_moments,
                                                                       h.d_pm_moments + (int64_t)Nk * Np, O, Od,
-                                                                      h.pm_cols > 1, h.d_pmU);
+                                                                      h.pm_cols > 1, h.d_U);
     else
         pm_velocity_kernel<float><<<blocks, PM_WARPS * 32, smem, s>>>((const float*)Nin, P, Nk, Np, h.d_pm_moments,
                                                                      h.d_pm_moments + (int64_t)Nk * Np, O, Od,
-                                                                     h.pm_cols > 1, h.d_pmU);
+                                                                     h.pm_cols > 1, h.d_U);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    pm_coef_kernel<<<blocks_for(c3, 256), 256, 0, s>>>(d.Nx, d.Ny, Nk, h.d_pmU, 1.0 / d.dx, 1.0 / d.dy, h.d_coef);
-    e = cudaGetLastError();
+    e = launch_coef_from_U(h, s);
     if (e == cudaSuccess) h.pm_ready = true;
     return e;
-}
-
-cudaError_t launch_pm_export(const Handle& h, cudaStream_t s) {
-    const int64_t c3 = h.cells * h.desc.Nk;
-    if (!h.pm_ready) return cudaMemsetAsync(h.d_coupling, 0, 8 * c3 * sizeof(double), s);
-    pm_export_kernel<<<blocks_for(c3, 256), 256, 0, s>>>(h.cells, (int)h.desc.Nk, h.d_pmU, h.d_coupling);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    return launch_gradients(h, s);
 }
 
 void free_pm(Handle* h) {
     const int64_t Nk = h->desc.Nk, Np = h->desc.Np;
     if (h->d_pm_overlap) h->bytes -= 2 * h->pm_cols * Nk * Nk * 8;
     if (h->d_pm_moments) h->bytes -= 2 * Nk * Np * 8;
-    if (h->d_pmU) h->bytes -= 4 * h->cells * Nk * 8;
-    for (double* p : {h->d_pm_overlap, h->d_pm_moments, h->d_pmU})
+    for (double* p : {h->d_pm_overlap, h->d_pm_moments})
         if (p) cudaFree(p);
-    h->d_pm_overlap = h->d_pm_moments = h->d_pmU = nullptr;
+    h->d_pm_overlap = h->d_pm_moments = nullptr;
     h->pm = h->pm_ready = false;
     h->pm_cols = 0;
 }
@@ -260,32 +216,36 @@ extern "C" int rpl_set_pseudomomentum(rpl_handle* hh, int64_t Nz, const double* 
     } else {
         return pm_fail(RPL_ERR_ARGUMENT, "Q-transform depth must be constant or a field");
     }
-    const int64_t table_bytes = 2 * cols * Nk * Nk * 8, moment_bytes = 2 * Nk * Np * 8, u_bytes = 4 * c3 * 8;
-    const int64_t extra = table_bytes + moment_bytes + u_bytes + (h->d_coupling ? 0 : 8 * c3 * 8);
+    const int64_t table_bytes = 2 * cols * Nk * Nk * 8, moment_bytes = 2 * Nk * Np * 8;
+    const int64_t extra = table_bytes + moment_bytes + (h->d_coupling ? 0 : 8 * c3 * 8) + (h->d_U ? 0 : 4 * c3 * 8);
     if (d.memory_limit_bytes > 0 && h->bytes + extra > d.memory_limit_bytes)
         return pm_fail(RPL_ERR_OOM, "pseudomomentum tables need " + std::to_string(extra) +
                                         " more device bytes, above the memory limit");
     cudaStream_t s = h->stream;
     e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return pm_fail(RPL_ERR_CUDA, std::string("rpl_set_pseudomomentum: ") + cudaGetErrorString(e));
-    // previous tables (another Q grid) go; the coupling buffers of prescribed currents stay allocated
+    // previous tables (another Q grid) and prescribed currents go; the coupling buffers stay allocated
     rpl::free_pm(h);
+    rpl::free_currents(h);
     if (!h->d_coupling) {
         e = cudaMalloc(&h->d_coupling, 8 * c3 * sizeof(double));
         if (e != cudaSuccess) return pm_fail(RPL_ERR_OOM, "pseudomomentum coupling: device allocation failed");
         h->bytes += 8 * c3 * 8;
     }
+    if (!h->d_U) {
+        e = cudaMalloc(&h->d_U, 4 * c3 * sizeof(double));
+        if (e != cudaSuccess) return pm_fail(RPL_ERR_OOM, "pseudomomentum coupling: device allocation failed");
+        h->bytes += 4 * c3 * 8;
+    }
     e = cudaMalloc(&h->d_pm_overlap, table_bytes);
     if (e == cudaSuccess) e = cudaMalloc(&h->d_pm_moments, moment_bytes);
-    if (e == cudaSuccess) e = cudaMalloc(&h->d_pmU, u_bytes);
     if (e == cudaSuccess) {
-        h->bytes += table_bytes + moment_bytes + u_bytes;
+        h->bytes += table_bytes + moment_bytes;
         h->pm_cols = cols;
     } else {
         cudaFree(h->d_pm_overlap);
         cudaFree(h->d_pm_moments);
-        cudaFree(h->d_pmU);
-        h->d_pm_overlap = h->d_pm_moments = h->d_pmU = nullptr;
+        h->d_pm_overlap = h->d_pm_moments = nullptr;
         cudaGetLastError();
         return pm_fail(RPL_ERR_OOM, "pseudomomentum tables: device allocation failed");
     }
@@ -317,6 +277,7 @@ extern "C" int rpl_set_pseudomomentum(rpl_handle* hh, int64_t Nz, const double* 
     }
     // the coupling starts at zero like the reference's caches (current_coupling.jl:103-107)
     if (e == cudaSuccess) e = cudaMemsetAsync(h->d_coupling, 0, 8 * c3 * sizeof(double), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(h->d_U, 0, 4 * c3 * sizeof(double), s);
     if (e == cudaSuccess) {
         h->currents_set = true;
         e = rpl::launch_coef(*h, s);

@@ -14,45 +14,95 @@ namespace rpl {
 
 namespace {
 
-// U[i,j,m] = sum_k uL[i,j,k] * (F(z_{k+1}) - F(z_k)) (doppler_velocity.jl:45-62) and the same sum with
-// dF/dkappa (:64-82). One warp per (i,j) column; lanes stride the vertical cells, the partial
-// sums meet in a warp-shuffle reduction.
+// Q weight of vertical cell k for ring m at column depth d (q_kernel.jl:87-116): F(z_k+1) - F(z_k), or
+// with derivative the same difference of dF/dkappa.
+__device__ __forceinline__ double q_weight(double kap, double lo, double hi, double d, double small_mu,
+                                           int exact_form, int derivative) {
+    return derivative ? q_cdf_dk(kap, hi, d, small_mu) - q_cdf_dk(kap, lo, d, small_mu)
+                      : q_cdf(kap, hi, d, small_mu, exact_form) - q_cdf(kap, lo, d, small_mu, exact_form);
+}
+
+// Q weights W[k,m] and Wd[k,m] of one constant projection depth, (Nz, Nk) with m fastest.
+__global__ void q_table_kernel(int64_t Nz, int64_t Nk, const double* __restrict__ zf, double d,
+                               const double* __restrict__ kappa, double small_mu, int exact_form,
+                               double* __restrict__ W, double* __restrict__ Wd) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= Nz * Nk) return;
+    const int64_t k = t / Nk, m = t - k * Nk;
+    const double kap = kappa[m], lo = zf[k], hi = zf[k + 1];
+    W[t] = q_weight(kap, lo, hi, d, small_mu, exact_form, 0);
+    Wd[t] = q_weight(kap, lo, hi, d, small_mu, exact_form, 1);
+}
+
+// Per-column Q weights of a depth field, column-contiguous (Nz, Nk) blocks with m fastest, stored as TW.
+// One warp per column, lanes over the rings; each lane walks the faces once (a face's F serves the two
+// cells that share it).
+template <typename TW>
+__global__ void q_column_table_kernel(int64_t P, int64_t Nz, int64_t Nk, const double* __restrict__ zf,
+                                      const double* __restrict__ qdepth, const double* __restrict__ kappa,
+                                      double small_mu, int exact_form, TW* __restrict__ W) {
+    const int lane = threadIdx.x & 31;
+    const int64_t col = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (col >= P) return;
+    const double d = qdepth[col];
+    TW* w = W + col * Nz * Nk;
+    for (int64_t m = lane; m < Nk; m += 32) {
+        const double kap = kappa[m];
+        double F0 = q_cdf(kap, zf[0], d, small_mu, exact_form);
+        for (int64_t k = 0; k < Nz; ++k) {
+            const double F1 = q_cdf(kap, zf[k + 1], d, small_mu, exact_form);
+            w[k * Nk + m] = (TW)(F1 - F0);
+            F0 = F1;
+        }
+    }
+}
+
+// U[i,j,m] = sum_k uL[i,j,k] * W_m[k] (doppler_velocity.jl:45-62; with derivative the dF/dkappa
+// weights of :64-82), sequential in k like the reference. One warp per (i,j) column, lanes over the
+// kappa rings (chunks of 32); u, v are warp-uniform loads; U is written in device order c*Nk + m
+// (coalesced). The weights come from a shared (Nz, Nk)
+// table (W, col_stride 0), a per-column table (col_stride Nz*Nk), or are evaluated here (W null; each
+// face once). z faces are strictly increasing (checked by the caller).
+template <typename TW>
 __global__ void doppler_kernel(int64_t Nx, int64_t Ny, int64_t Nz, int64_t Nk,
                                const double* __restrict__ u, const double* __restrict__ v,
                                const double* __restrict__ zf, const double* __restrict__ qdepth,
                                double qdepth_const, const double* __restrict__ kappa, double small_mu,
-                               int exact_form, double* __restrict__ Ux, double* __restrict__ Uy,
-                               double* __restrict__ dUx, double* __restrict__ dUy) {
+                               int exact_form, int derivative, const TW* __restrict__ W, int64_t col_stride,
+                               double* __restrict__ Ux, double* __restrict__ Uy) {
     const int lane = threadIdx.x & 31;
     const int64_t col = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (col >= Nx * Ny) return;
-    const double d = qdepth ? qdepth[col] : qdepth_const;
     const int64_t P = Nx * Ny;
-    for (int64_t m = 0; m < Nk; ++m) {
-        const double kap = kappa[m];
-        double ax = 0.0, ay = 0.0, bx = 0.0, by = 0.0;
-        for (int64_t k = lane; k < Nz; k += 32) {
-            const double lo = fmin(zf[k], zf[k + 1]), hi = fmax(zf[k], zf[k + 1]);
-            const double w = q_cdf(kap, hi, d, small_mu, exact_form) - q_cdf(kap, lo, d, small_mu, exact_form);
-            const double wd = q_cdf_dk(kap, hi, d, small_mu) - q_cdf_dk(kap, lo, d, small_mu);
-            const double uu = u[col + P * k], vv = v[col + P * k];
-            ax += uu * w;
-            ay += vv * w;
-            bx += uu * wd;
-            by += vv * wd;
+    if (col >= P) return;
+    const double d = qdepth ? qdepth[col] : qdepth_const;
+    for (int64_t m0 = 0; m0 < Nk; m0 += 32) {
+        const int64_t m = m0 + lane;
+        const bool active = m < Nk;
+        const int64_t mm = active ? m : Nk - 1;
+        double ax = 0.0, ay = 0.0;
+        if (W) {
+            const TW* w = W + col * col_stride + mm;
+#pragma unroll 4
+            for (int64_t k = 0; k < Nz; ++k) {
+                const double wk = (double)__ldg(w + k * Nk);
+                ax += __ldg(u + col + P * k) * wk;
+                ay += __ldg(v + col + P * k) * wk;
+            }
+        } else {
+            const double kap = kappa[mm];
+            double F0 = derivative ? q_cdf_dk(kap, zf[0], d, small_mu) : q_cdf(kap, zf[0], d, small_mu, exact_form);
+            for (int64_t k = 0; k < Nz; ++k) {
+                const double z1 = zf[k + 1];
+                const double F1 = derivative ? q_cdf_dk(kap, z1, d, small_mu) : q_cdf(kap, z1, d, small_mu, exact_form);
+                const double wk = F1 - F0;
+                ax += __ldg(u + col + P * k) * wk;
+                ay += __ldg(v + col + P * k) * wk;
+                F0 = F1;
+            }
         }
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) {
-            ax += __shfl_down_sync(0xffffffffu, ax, off);
-            ay += __shfl_down_sync(0xffffffffu, ay, off);
-            bx += __shfl_down_sync(0xffffffffu, bx, off);
-            by += __shfl_down_sync(0xffffffffu, by, off);
-        }
-        if (lane == 0) {
-            Ux[col + P * m] = ax;
-            Uy[col + P * m] = ay;
-            dUx[col + P * m] = bx;
-            dUy[col + P * m] = by;
+        if (active) {
+            Ux[col * Nk + m] = ax;
+            Uy[col * Nk + m] = ay;
         }
     }
 }
@@ -258,16 +308,51 @@ inline unsigned blocks_for(int64_t n, int threads) { return (unsigned)((n + thre
 
 }  // namespace
 
-cudaError_t launch_doppler(const Handle& h, int64_t Nz, const double* d_u, const double* d_v,
-                           const double* d_zf, const double* d_qdepth, double qdepth_const,
-                           double small_mu, cudaStream_t s) {
-    const rpl_desc& d = h.desc;
-    const int64_t c3 = d.Nx * d.Ny * d.Nk;
-    const int64_t cols = d.Nx * d.Ny;
+cudaError_t launch_q_table(const Handle& h, int64_t Nz, const double* d_zf, double qdepth_const, double small_mu,
+                           double* W, double* Wd, cudaStream_t s) {
+    const int64_t n = Nz * h.desc.Nk;
     const int exact_form = h.precision == RPL_FP64 ? 1 : 0;
-    doppler_kernel<<<blocks_for(cols * 32, 256), 256, 0, s>>>(
-        d.Nx, d.Ny, Nz, d.Nk, d_u, d_v, d_zf, d_qdepth, qdepth_const, h.d_kappa, small_mu, exact_form,
-        h.d_coupling, h.d_coupling + c3, h.d_coupling + 2 * c3, h.d_coupling + 3 * c3);
+    q_table_kernel<<<blocks_for(n, 256), 256, 0, s>>>(Nz, h.desc.Nk, d_zf, qdepth_const, h.d_kappa, small_mu,
+                                                      exact_form, W, Wd);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_q_column_table(const Handle& h, cudaStream_t s) {
+    const int64_t P = h.cells;
+    const int exact_form = h.precision == RPL_FP64 ? 1 : 0;
+    if (h.q_col_f32)
+        q_column_table_kernel<float><<<blocks_for(P * 32, 256), 256, 0, s>>>(
+            P, h.q_Nz, h.desc.Nk, h.d_qz, h.d_qdepth, h.d_kappa, h.q_small_mu, exact_form, (float*)h.d_qcol);
+    else
+        q_column_table_kernel<double><<<blocks_for(P * 32, 256), 256, 0, s>>>(
+            P, h.q_Nz, h.desc.Nk, h.d_qz, h.d_qdepth, h.d_kappa, h.q_small_mu, exact_form, (double*)h.d_qcol);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_doppler(const Handle& h, const double* d_u, const double* d_v, int derivative, double* Ux,
+                           double* Uy, cudaStream_t s) {
+    const rpl_desc& d = h.desc;
+    const int64_t cols = d.Nx * d.Ny, Nz = h.q_Nz, tab = Nz * d.Nk;
+    const int exact_form = h.precision == RPL_FP64 ? 1 : 0;
+    const unsigned blocks = blocks_for(cols * 32, 256);
+    if (h.d_qW) {  // constant projection depth: shared tables
+        doppler_kernel<double><<<blocks, 256, 0, s>>>(d.Nx, d.Ny, Nz, d.Nk, d_u, d_v, h.d_qz, nullptr, h.q_const,
+                                                      h.d_kappa, h.q_small_mu, exact_form, derivative,
+                                                      h.d_qW + (derivative ? tab : 0), 0, Ux, Uy);
+    } else if (h.d_qcol && !derivative) {  // depth field with cached per-column weights
+        if (h.q_col_f32)
+            doppler_kernel<float><<<blocks, 256, 0, s>>>(d.Nx, d.Ny, Nz, d.Nk, d_u, d_v, h.d_qz, h.d_qdepth, 0.0,
+                                                         h.d_kappa, h.q_small_mu, exact_form, 0,
+                                                         (const float*)h.d_qcol, tab, Ux, Uy);
+        else
+            doppler_kernel<double><<<blocks, 256, 0, s>>>(d.Nx, d.Ny, Nz, d.Nk, d_u, d_v, h.d_qz, h.d_qdepth, 0.0,
+                                                          h.d_kappa, h.q_small_mu, exact_form, 0,
+                                                          (const double*)h.d_qcol, tab, Ux, Uy);
+    } else {  // depth field, weights evaluated per column
+        doppler_kernel<double><<<blocks, 256, 0, s>>>(d.Nx, d.Ny, Nz, d.Nk, d_u, d_v, h.d_qz, h.d_qdepth, 0.0,
+                                                      h.d_kappa, h.q_small_mu, exact_form, derivative, nullptr, 0,
+                                                      Ux, Uy);
+    }
     return cudaGetLastError();
 }
 

@@ -83,6 +83,8 @@ _SIGNATURES = {
     "rpl_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "rpl_set_currents": (ctypes.c_int, [ctypes.c_void_p, _i64, _dp, _i32, _d, _dp, _dp, _dp, _d]),
     "rpl_get_coupling": (ctypes.c_int, [ctypes.c_void_p] + [_dp] * 8),
+    "rpl_update_currents": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp]),
+    "rpl_update_currents_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "rpl_set_pseudomomentum": (ctypes.c_int, [ctypes.c_void_p, _i64, _dp, _i32, _d, _dp, _d]),
     "rpl_update_coupling": (ctypes.c_int, [ctypes.c_void_p]),
     "rpl_set_sources": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(RplSources)]),

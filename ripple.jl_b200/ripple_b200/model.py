@@ -330,9 +330,43 @@ class SpectralWaveModel:
         self._q = dict(zfaces=zf, kind=qkind, const=qconst, field=qfield)
 
     def update_coupling(self):
-        """update_coupling!(model) (current_coupling.jl:140-148): recompute a pseudomomentum coupling from
-        the current action (prescribed currents are static)."""
-        check(self._lib.rpl_update_coupling(self._h))
+        """update_coupling!(model) (current_coupling.jl:127-148): a pseudomomentum coupling is recomputed
+        from the current action; prescribed currents are re-read from `velocities` (its "u" and "v" entries,
+        arrays or callables of (x, y, z)) and projected again, as the reference re-reads its current fields."""
+        if isinstance(self.velocities, dict) and self._transport == _lib.RPL_TRANSPORT_REFRACTION:
+            self.update_currents(self.velocities["u"], self.velocities["v"])
+        else:
+            check(self._lib.rpl_update_coupling(self._h))
+        return self
+
+    def _current_arrays(self, u, v):
+        q = self.q_grid
+        if callable(u) or callable(v):
+            X, Y, Z = np.meshgrid(q.xnodes(), q.ynodes(), q.znodes(), indexing="ij")
+        uu = np.broadcast_to(np.asarray(u(X, Y, Z), dtype=np.float64), X.shape) if callable(u) else np.asarray(u, np.float64)
+        vv = np.broadcast_to(np.asarray(v(X, Y, Z), dtype=np.float64), X.shape) if callable(v) else np.asarray(v, np.float64)
+        shape = (self.grid.Nx, self.grid.Ny, q.Nz)
+        if uu.shape != shape or vv.shape != shape:
+            raise ArgumentError(f"u and v must have size {shape}")
+        return _xfast(uu), _xfast(vv)
+
+    def update_currents(self, u, v):
+        """New prescribed currents on the Q grid of the model's velocities, applied from the next step on
+        without allocating on the device (time-varying currents). u, v: (Nx, Ny, Nz) arrays or callables;
+        or float64 CUDA tensors of that shape with x fastest (stride (1, Nx, Nx*Ny)), read in place."""
+        if getattr(self, "_u", None) is None:
+            raise ArgumentError("update_currents needs prescribed velocities")
+        if hasattr(u, "data_ptr") and getattr(u, "is_cuda", False):
+            Nx, Ny = self.grid.Nx, self.grid.Ny
+            for t in (u, v):
+                if (str(t.dtype) != "torch.float64" or tuple(t.shape) != (Nx, Ny, self.q_grid.Nz)
+                        or tuple(t.stride()) != (1, Nx, Nx * Ny)):
+                    raise ArgumentError("device currents must be float64 (Nx, Ny, Nz) tensors with x fastest")
+            check(self._lib.rpl_update_currents_device(self._h, _lib.ctypes.c_void_p(u.data_ptr()),
+                                                       _lib.ctypes.c_void_p(v.data_ptr())))
+            return self
+        self._u, self._v = self._current_arrays(u, v)
+        check(self._lib.rpl_update_currents(self._h, dptr(self._u), dptr(self._v)))
         return self
 
     def _set_velocities(self, velocities):

@@ -180,7 +180,7 @@ def hurricane_swell(N=768, Nk=32, Np=36, nsteps=1000, L=768 * 10000.0, cfl=0.4, 
 
 
 def self_coupled_swell(N=64, Nk=16, Np=24, nsteps=200, dx=2000.0, depth=50.0, depth_field=False, amplitude=4e4,
-                       seed=7, cfl=0.4, peak_velocity=0.3):
+                       seed=7, cfl=0.4, peak_velocity=0.3, n0_dtype=np.float64):
     """PseudomomentumVelocities: a swell packet whose own pseudomomentum Doppler-shifts it. Flat periodic
     N x N grid at dx; 16 log kappa 0.01-0.3 x 24 directions; finite depth (50 m, or with depth_field a
     seeded 30-80 m bathymetry) so the Q grid is the automatic stretched one; N0 = amplitude x Gaussian
@@ -204,7 +204,10 @@ def self_coupled_swell(N=64, Nk=16, Np=24, nsteps=200, dx=2000.0, depth=50.0, de
     K, P = np.meshgrid(kappa, phi, indexing="ij")
     spec = np.exp(-((np.log(K / 0.05)) / 0.3) ** 2) * np.cos((P - 0.5) / 2) ** 20
     env = np.exp(-((X - L / 2) ** 2 + (Y - L / 2) ** 2) / (2 * (L / 6) ** 2))
-    N0 = np.asfortranarray(amplitude * env[:, :, None, None] * spec[None, None] + 1e-3)
+    N0 = np.empty((N, N, Nk, Np), dtype=n0_dtype, order="F")
+    for n in range(Np):
+        for m in range(Nk):
+            N0[:, :, m, n] = amplitude * spec[m, n] * env + 1e-3
     hmax = float(np.max(depth))
     cg_max = max(0.5 * math.sqrt(G * math.tanh(k * hmax) / k) for k in kappa) + peak_velocity
     grad = 2.0 * peak_velocity / (L / 6)
