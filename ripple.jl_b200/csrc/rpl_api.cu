@@ -148,7 +148,7 @@ int launch_step(Handle* h, double dt, int stage_only) {
             if (h->learned) RPL_CUDA(rpl::launch_learned_stage_prep(*h, Nin, s));
             else if (h->src.stress_cap) RPL_CUDA(rpl::launch_stress_factor(*h, Nin, s));
         }
-        if (h->pm) RPL_CUDA(rpl::launch_pm_refresh(*h, Nin, s));
+        if (h->pm) RPL_CUDA(rpl::launch_pm_refresh(*h, Nin, s, false));
         const rpl::StageParams p = rpl::make_params(*h, dt, stage);
         RPL_CUDA(rpl::launch_stage(*h, p, Nin, h->N, Nout, s));
     }
@@ -507,6 +507,10 @@ int rpl_get_coupling(rpl_handle* hh, double* Ux, double* Uy, double* dUxdk, doub
     Handle* h = reinterpret_cast<Handle*>(hh);
     if (!h->currents_set) return fail(RPL_ERR_STATE, "no currents set");
     const int64_t c3 = h->desc.Nx * h->desc.Ny * h->desc.Nk;
+    if (h->pm && h->dU_stale) {
+        RPL_CUDA(rpl::launch_pm_derivative(*h, h->stream));
+        h->dU_stale = false;
+    }
     if (!h->pm && h->dU_stale) {
         const int64_t n3 = h->cells * h->q_Nz;
         RPL_CUDA(rpl::launch_doppler(*h, h->d_cur, h->d_cur + n3, 1, h->d_U + 2 * c3, h->d_U + 3 * c3, h->stream));
@@ -801,7 +805,7 @@ int rpl_tendency(rpl_handle* hh, double* G, int32_t layout) {
         e = rpl::launch_wind(*h, h->time, s);
         if (e == cudaSuccess && h->src.stress_cap) e = rpl::launch_stress_factor(*h, h->N, s);
     }
-    if (e == cudaSuccess && h->pm) e = rpl::launch_pm_refresh(*h, h->N, s);
+    if (e == cudaSuccess && h->pm) e = rpl::launch_pm_refresh(*h, h->N, s, true);
     if (e == cudaSuccess) e = rpl::launch_tendency(*h, rpl::make_params(*h, 1.0, 1), h->N, dG, s);
     if (e == cudaSuccess)
         e = rpl::launch_from_device_layout(*h, dG, RPL_F64, dGx, RPL_F64, 0, h->desc.Np, 0, h->desc.Nk, s);

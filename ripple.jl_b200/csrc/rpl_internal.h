@@ -144,13 +144,16 @@ struct Handle {
     double* d_cur = nullptr;       // u then v, (Nx,Ny,Nz) each, x fastest
     void* d_qcol = nullptr;        // depth field: per-column Q weights (Nz, Nk) per column, when memory allows
     bool q_col_f32 = false;        // d_qcol holds floats (FP32 models)
-    bool dU_stale = false;         // the dU/dkappa caches lag the last currents (computed on request)
+    bool dU_stale = false;         // the dU/dkappa caches lag the last currents or action (computed on request)
     // PseudomomentumVelocities (rpl_pm.cu)
     bool pm = false;               // the coupling is recomputed from the action before every stage
     bool pm_ready = false;         // d_U holds the velocity of some action
     int64_t pm_cols = 0;           // overlap table pairs: 1 (constant projection depth) or Nx*Ny
     double* d_pm_overlap = nullptr;  // overlap then derivative overlap, pm_cols x Nk x Nk each
     double* d_pm_moments = nullptr;  // kx then ky first-moment measures, (Nk, Np) m fastest
+    float* d_pm_overlap32 = nullptr;  // FP32 models: FP32 copy of the overlap table(s)
+    float* d_pm_moments32 = nullptr;  // FP32 models: FP32 copy of the moment measures
+    const void* pm_last_in = nullptr;  // the action of the last refresh (a state buffer)
     // sources
     rpl_sources src{};
     bool has_sources = false;
@@ -175,7 +178,10 @@ void free_learned(Handle* h);
 
 // Pseudomomentum self-coupling (rpl_pm.cu): refresh the velocity and coefficient records from the
 // action Nin; write the caller-order coupling arrays and their gradients into d_coupling; release.
-cudaError_t launch_pm_refresh(Handle& h, const void* Nin, cudaStream_t s);
+// Refresh of the Doppler velocity from the action Nin (with_derivative: dU/dkappa too, else on request).
+cudaError_t launch_pm_refresh(Handle& h, const void* Nin, cudaStream_t s, bool with_derivative);
+// dU/dkappa of the last refreshed action into d_U arrays 2-3 (zeros before any refresh).
+cudaError_t launch_pm_derivative(const Handle& h, cudaStream_t s);
 void free_pm(Handle* h);
 // Releases the prescribed-currents state of rpl_set_currents (rpl_api.cu).
 void free_currents(Handle* h);

@@ -80,27 +80,36 @@ __global__ void coef_kernel(int64_t Nx, int64_t Ny, int64_t Nk, const double* __
     r[7] = kappa[m];
 }
 
-// Coefficient records (Ux, Uy, Ux_x, Ux_y, Uy_x, Uy_y; fields 6 and 7 stay) from the device-order
-// velocity, with the periodic centred gradients of wave_current_refraction.jl:7-19.
-__global__ void coef_from_U_kernel(int64_t Nx, int64_t Ny, int Nk, const double* __restrict__ U, double dx_inv,
-                               double dy_inv, double* __restrict__ coef) {
-    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+constexpr int COEF_THREADS = 256;
+
+// Coefficient records (Ux, Uy, Ux_x, Ux_y, Uy_x, Uy_y; fields 6 and 7 are kept) from the device-order
+// velocity, with the periodic centred gradients of wave_current_refraction.jl:7-19. A block's 256
+// records are assembled in shared memory and written back whole with 16-byte stores, so every DRAM
+// sector is written in full.
+__global__ void __launch_bounds__(COEF_THREADS)
+coef_from_U_kernel(int64_t Nx, int64_t Ny, int Nk, const double* __restrict__ U, double dx_inv, double dy_inv,
+                   double* __restrict__ coef) {
+    __shared__ double2 rec[COEF_THREADS * 4];
     const int64_t P = Nx * Ny, c3 = P * Nk;
-    if (t >= c3) return;
-    const int64_t c = t / Nk, m = t - c * Nk;
-    const int64_t j = c / Nx, i = c - j * Nx;
-    const int64_t ip = i == Nx - 1 ? 0 : i + 1, im = i == 0 ? Nx - 1 : i - 1;
-    const int64_t jp = j == Ny - 1 ? 0 : j + 1, jm = j == 0 ? Ny - 1 : j - 1;
-    const int64_t xp = (j * Nx + ip) * Nk + m, xm = (j * Nx + im) * Nk + m;
-    const int64_t yp = (jp * Nx + i) * Nk + m, ym = (jm * Nx + i) * Nk + m;
-    const double* Uy = U + c3;
-    double* r = coef + 8 * t;
-    r[0] = U[t];
-    r[1] = Uy[t];
-    r[2] = (U[xp] - U[xm]) * (dx_inv / 2.0);
-    r[3] = (U[yp] - U[ym]) * (dy_inv / 2.0);
-    r[4] = (Uy[xp] - Uy[xm]) * (dx_inv / 2.0);
-    r[5] = (Uy[yp] - Uy[ym]) * (dy_inv / 2.0);
+    const int64_t t0 = (int64_t)blockIdx.x * COEF_THREADS, t = t0 + threadIdx.x;
+    if (t < c3) {
+        const int64_t c = t / Nk, m = t - c * Nk;
+        const int64_t j = c / Nx, i = c - j * Nx;
+        const int64_t ip = i == Nx - 1 ? 0 : i + 1, im = i == 0 ? Nx - 1 : i - 1;
+        const int64_t jp = j == Ny - 1 ? 0 : j + 1, jm = j == 0 ? Ny - 1 : j - 1;
+        const int64_t xp = (j * Nx + ip) * Nk + m, xm = (j * Nx + im) * Nk + m;
+        const int64_t yp = (jp * Nx + i) * Nk + m, ym = (jm * Nx + i) * Nk + m;
+        const double* Uy = U + c3;
+        double2* r = rec + threadIdx.x * 4;
+        r[0] = make_double2(U[t], Uy[t]);
+        r[1] = make_double2((U[xp] - U[xm]) * (dx_inv / 2.0), (U[yp] - U[ym]) * (dy_inv / 2.0));
+        r[2] = make_double2((Uy[xp] - Uy[xm]) * (dx_inv / 2.0), (Uy[yp] - Uy[ym]) * (dy_inv / 2.0));
+        r[3] = *reinterpret_cast<const double2*>(coef + 8 * t + 6);
+    }
+    __syncthreads();
+    const int n = (int)(min((int64_t)COEF_THREADS, c3 - t0) * 4);
+    double2* out = reinterpret_cast<double2*>(coef + 8 * t0);
+    for (int k = threadIdx.x; k < n; k += COEF_THREADS) out[k] = rec[k];
 }
 
 // Device-order velocity -> the caller-order coupling arrays Ux, Uy, dUx/dkappa, dUy/dkappa (x fastest).
@@ -161,8 +170,8 @@ cudaError_t launch_coef(const Handle& h, cudaStream_t s) {
 cudaError_t launch_coef_from_U(const Handle& h, cudaStream_t s) {
     const rpl_desc& d = h.desc;
     const int64_t c3 = d.Nx * d.Ny * d.Nk;
-    coef_from_U_kernel<<<(unsigned)((c3 + 255) / 256), 256, 0, s>>>(d.Nx, d.Ny, (int)d.Nk, h.d_U, 1.0 / d.dx,
-                                                                    1.0 / d.dy, h.d_coef);
+    coef_from_U_kernel<<<(unsigned)((c3 + COEF_THREADS - 1) / COEF_THREADS), COEF_THREADS, 0, s>>>(
+        d.Nx, d.Ny, (int)d.Nk, h.d_U, 1.0 / d.dx, 1.0 / d.dy, h.d_coef);
     return cudaGetLastError();
 }
 

@@ -3,8 +3,9 @@
 // src/Coupling/pseudomomentum.jl:68-138,316-342, src/Coupling/lagrangian_velocities.jl:294-311).
 //
 // Set-up builds the vertical overlap tables of the Q transform once (one Nk x Nk pair for a constant
-// projection depth, one pair per (i,j) column for a depth field). Before every RK3 stage (and every
-// stand-alone tendency) the coupling is refreshed from the stage's input action:
+// projection depth, one pair per (i,j) column for a depth field; FP32 copies for FP32 models). Before
+// every RK3 stage (and every stand-alone tendency) the Doppler velocity is refreshed from the stage's
+// input action (dU/dkappa, which the stage kernels do not read, follows on request):
 //   pm_velocity_kernel  one warp per (i,j) column: first moments M_s = sum_n N[s,n] k_measure[s,n]
 //                       for every source ring s (lanes over s, coalesced kappa-contiguous reads of the
 //                       state), then U_t = sum_s overlap[t,s] M_s and dU/dkappa_t with the derivative
@@ -80,25 +81,26 @@ __global__ void pm_overlap_kernel(int Nk, int64_t Nz, int kc_max, const double* 
 }
 
 // Doppler velocity of the pseudomomentum (pseudomomentum.jl:316-342), one warp per (i,j) column.
-// N: device layout (n*P + c)*Nk + m. kx, ky: (Nk, Np) first-moment measures, m fastest. O, Od: one
-// table pair (per_cell = 0) or one per column. U: Ux, Uy, dUx/dkappa, dUy/dkappa, each c3 doubles in
-// device order c*Nk + t.
-template <typename T>
+// N: device layout (n*P + c)*Nk + m. kx, ky: (Nk, Np) first-moment measures, m fastest. O: the overlap
+// table (or the derivative overlap, for dU/dkappa), one Nk x Nk table (per_cell = 0) or one per column.
+// Ux, Uy: c3 doubles each in device order c*Nk + t. A is the arithmetic type: double for FP64 models
+// and for dU/dkappa, float for the per-stage refresh of FP32 models.
+template <typename T, typename A>
 __global__ void __launch_bounds__(PM_WARPS * 32)
-pm_velocity_kernel(const T* __restrict__ N, int64_t P, int Nk, int Np, const double* __restrict__ kx,
-                   const double* __restrict__ ky, const double* __restrict__ O, const double* __restrict__ Od,
-                   int per_cell, double* __restrict__ U) {
-    extern __shared__ double sm[];
+pm_velocity_kernel(const T* __restrict__ N, int64_t P, int Nk, int Np, const A* __restrict__ kx,
+                   const A* __restrict__ ky, const A* __restrict__ O, int per_cell, double* __restrict__ Ux,
+                   double* __restrict__ Uy) {
+    extern __shared__ __align__(16) unsigned char pm_smem[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int64_t c = (int64_t)blockIdx.x * PM_WARPS + w;
     if (c >= P) return;  // uniform per warp; the kernel has no block-wide barrier
-    double* mx = sm + (int64_t)w * 2 * Nk;
-    double* my = mx + Nk;
+    A* mx = reinterpret_cast<A*>(pm_smem) + (int64_t)w * 2 * Nk;
+    A* my = mx + Nk;
     for (int s = lane; s < Nk; s += 32) {
-        double ax = 0.0, ay = 0.0;
-#pragma unroll 4
+        A ax = 0, ay = 0;
+#pragma unroll 6
         for (int n = 0; n < Np; ++n) {
-            const double a = (double)N[((int64_t)n * P + c) * Nk + s];
+            const A a = (A)N[((int64_t)n * P + c) * Nk + s];
             ax += a * __ldg(kx + s + (int64_t)Nk * n);
             ay += a * __ldg(ky + s + (int64_t)Nk * n);
         }
@@ -106,26 +108,24 @@ pm_velocity_kernel(const T* __restrict__ N, int64_t P, int Nk, int Np, const dou
         my[s] = ay;
     }
     __syncwarp();
-    const int64_t n2 = (int64_t)Nk * Nk;
-    const double* o = per_cell ? O + c * n2 : O;
-    const double* od = per_cell ? Od + c * n2 : Od;
-    const int64_t c3 = P * Nk;
+    const A* o = per_cell ? O + c * (int64_t)Nk * Nk : O;
     for (int t = lane; t < Nk; t += 32) {
-        double ux = 0.0, uy = 0.0, dx = 0.0, dy = 0.0;
+        A ux = 0, uy = 0;
+#pragma unroll 8
         for (int s = 0; s < Nk; ++s) {
-            const double q = __ldg(o + (int64_t)s * Nk + t), dq = __ldg(od + (int64_t)s * Nk + t);
-            const double a = mx[s], b = my[s];
-            ux += q * a;
-            uy += q * b;
-            dx += dq * a;
-            dy += dq * b;
+            const A q = __ldg(o + (int64_t)s * Nk + t);
+            ux += q * mx[s];
+            uy += q * my[s];
         }
-        const int64_t x = c * Nk + t;
-        U[x] = ux;
-        U[c3 + x] = uy;
-        U[2 * c3 + x] = dx;
-        U[3 * c3 + x] = dy;
+        Ux[c * Nk + t] = (double)ux;
+        Uy[c * Nk + t] = (double)uy;
     }
+}
+
+// FP32 copy of a table.
+__global__ void to_f32_kernel(const double* __restrict__ a, int64_t n, float* __restrict__ b) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) b[t] = (float)a[t];
 }
 
 inline unsigned blocks_for(int64_t n, int threads) { return (unsigned)((n + threads - 1) / threads); }
@@ -134,36 +134,64 @@ int overlap_chunk(int Nk) { return std::max(1, std::min(32, 2048 / Nk)); }
 
 }  // namespace
 
-cudaError_t launch_pm_refresh(Handle& h, const void* Nin, cudaStream_t s) {
+cudaError_t launch_pm_refresh(Handle& h, const void* Nin, cudaStream_t s, bool with_derivative) {
     const rpl_desc& d = h.desc;
     const int Nk = (int)d.Nk, Np = (int)d.Np;
-    const int64_t P = h.cells;
-    const size_t smem = (size_t)PM_WARPS * 2 * Nk * sizeof(double);
+    const int64_t P = h.cells, c3 = P * Nk;
     const unsigned blocks = blocks_for(P, PM_WARPS);
-    const double* O = h.d_pm_overlap;
-    const double* Od = h.d_pm_overlap + h.pm_cols * (int64_t)Nk * Nk;
     if (h.precision == RPL_FP64)
-        pm_velocity_kernel<double><<<blocks, PM_WARPS * 32, smem, s>>>((const double*)Nin, P, Nk, Np, h.d_pm_moments,
-                                                                      h.d_pm_moments + (int64_t)Nk * Np, O, Od,
-                                                                      h.pm_cols > 1, h.d_U);
+        pm_velocity_kernel<double, double><<<blocks, PM_WARPS * 32, (size_t)PM_WARPS * 2 * Nk * 8, s>>>(
+            (const double*)Nin, P, Nk, Np, h.d_pm_moments, h.d_pm_moments + (int64_t)Nk * Np, h.d_pm_overlap,
+            h.pm_cols > 1, h.d_U, h.d_U + c3);
     else
-        pm_velocity_kernel<float><<<blocks, PM_WARPS * 32, smem, s>>>((const float*)Nin, P, Nk, Np, h.d_pm_moments,
-                                                                     h.d_pm_moments + (int64_t)Nk * Np, O, Od,
-                                                                     h.pm_cols > 1, h.d_U);
+        pm_velocity_kernel<float, float><<<blocks, PM_WARPS * 32, (size_t)PM_WARPS * 2 * Nk * 4, s>>>(
+            (const float*)Nin, P, Nk, Np, h.d_pm_moments32, h.d_pm_moments32 + (int64_t)Nk * Np, h.d_pm_overlap32,
+            h.pm_cols > 1, h.d_U, h.d_U + c3);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     e = launch_coef_from_U(h, s);
-    if (e == cudaSuccess) h.pm_ready = true;
+    if (e != cudaSuccess) return e;
+    h.pm_ready = true;
+    h.pm_last_in = Nin;  // a state buffer that only the next step overwrites
+    h.dU_stale = true;
+    if (with_derivative) {
+        e = launch_pm_derivative(h, s);
+        if (e == cudaSuccess) h.dU_stale = false;
+    }
     return e;
+}
+
+cudaError_t launch_pm_derivative(const Handle& h, cudaStream_t s) {
+    const rpl_desc& d = h.desc;
+    const int Nk = (int)d.Nk, Np = (int)d.Np;
+    const int64_t P = h.cells, c3 = P * Nk;
+    if (!h.pm_ready) return cudaMemsetAsync(h.d_U + 2 * c3, 0, 2 * c3 * sizeof(double), s);
+    const unsigned blocks = blocks_for(P, PM_WARPS);
+    const size_t smem = (size_t)PM_WARPS * 2 * Nk * 8;
+    const double* Od = h.d_pm_overlap + h.pm_cols * (int64_t)Nk * Nk;
+    if (h.precision == RPL_FP64)
+        pm_velocity_kernel<double, double><<<blocks, PM_WARPS * 32, smem, s>>>(
+            (const double*)h.pm_last_in, P, Nk, Np, h.d_pm_moments, h.d_pm_moments + (int64_t)Nk * Np, Od,
+            h.pm_cols > 1, h.d_U + 2 * c3, h.d_U + 3 * c3);
+    else
+        pm_velocity_kernel<float, double><<<blocks, PM_WARPS * 32, smem, s>>>(
+            (const float*)h.pm_last_in, P, Nk, Np, h.d_pm_moments, h.d_pm_moments + (int64_t)Nk * Np, Od,
+            h.pm_cols > 1, h.d_U + 2 * c3, h.d_U + 3 * c3);
+    return cudaGetLastError();
 }
 
 void free_pm(Handle* h) {
     const int64_t Nk = h->desc.Nk, Np = h->desc.Np;
     if (h->d_pm_overlap) h->bytes -= 2 * h->pm_cols * Nk * Nk * 8;
     if (h->d_pm_moments) h->bytes -= 2 * Nk * Np * 8;
+    if (h->d_pm_overlap32) h->bytes -= h->pm_cols * Nk * Nk * 4 + 2 * Nk * Np * 4;
     for (double* p : {h->d_pm_overlap, h->d_pm_moments})
         if (p) cudaFree(p);
+    for (float* p : {h->d_pm_overlap32, h->d_pm_moments32})
+        if (p) cudaFree(p);
     h->d_pm_overlap = h->d_pm_moments = nullptr;
+    h->d_pm_overlap32 = h->d_pm_moments32 = nullptr;
+    h->pm_last_in = nullptr;
     h->pm = h->pm_ready = false;
     h->pm_cols = 0;
 }
@@ -216,8 +244,11 @@ extern "C" int rpl_set_pseudomomentum(rpl_handle* hh, int64_t Nz, const double* 
     } else {
         return pm_fail(RPL_ERR_ARGUMENT, "Q-transform depth must be constant or a field");
     }
+    const bool f32 = h->precision == RPL_FP32;
     const int64_t table_bytes = 2 * cols * Nk * Nk * 8, moment_bytes = 2 * Nk * Np * 8;
-    const int64_t extra = table_bytes + moment_bytes + (h->d_coupling ? 0 : 8 * c3 * 8) + (h->d_U ? 0 : 4 * c3 * 8);
+    const int64_t f32_bytes = f32 ? cols * Nk * Nk * 4 + 2 * Nk * Np * 4 : 0;
+    const int64_t extra = table_bytes + moment_bytes + f32_bytes + (h->d_coupling ? 0 : 8 * c3 * 8) +
+                          (h->d_U ? 0 : 4 * c3 * 8);
     if (d.memory_limit_bytes > 0 && h->bytes + extra > d.memory_limit_bytes)
         return pm_fail(RPL_ERR_OOM, "pseudomomentum tables need " + std::to_string(extra) +
                                         " more device bytes, above the memory limit");
@@ -239,13 +270,18 @@ extern "C" int rpl_set_pseudomomentum(rpl_handle* hh, int64_t Nz, const double* 
     }
     e = cudaMalloc(&h->d_pm_overlap, table_bytes);
     if (e == cudaSuccess) e = cudaMalloc(&h->d_pm_moments, moment_bytes);
+    if (e == cudaSuccess && f32) e = cudaMalloc(&h->d_pm_overlap32, cols * Nk * Nk * 4);
+    if (e == cudaSuccess && f32) e = cudaMalloc(&h->d_pm_moments32, 2 * Nk * Np * 4);
     if (e == cudaSuccess) {
-        h->bytes += table_bytes + moment_bytes;
+        h->bytes += table_bytes + moment_bytes + f32_bytes;
         h->pm_cols = cols;
     } else {
-        cudaFree(h->d_pm_overlap);
-        cudaFree(h->d_pm_moments);
+        for (double* p : {h->d_pm_overlap, h->d_pm_moments})
+            if (p) cudaFree(p);
+        for (float* p : {h->d_pm_overlap32, h->d_pm_moments32})
+            if (p) cudaFree(p);
         h->d_pm_overlap = h->d_pm_moments = nullptr;
+        h->d_pm_overlap32 = h->d_pm_moments32 = nullptr;
         cudaGetLastError();
         return pm_fail(RPL_ERR_OOM, "pseudomomentum tables: device allocation failed");
     }
@@ -275,6 +311,12 @@ extern "C" int rpl_set_pseudomomentum(rpl_handle* hh, int64_t Nz, const double* 
                                                                  h->d_pm_overlap, h->d_pm_overlap + cols * Nk * Nk);
         e = cudaGetLastError();
     }
+    if (e == cudaSuccess && f32) {
+        const int64_t n = cols * Nk * Nk, nm = 2 * Nk * Np;
+        rpl::to_f32_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(h->d_pm_overlap, n, h->d_pm_overlap32);
+        rpl::to_f32_kernel<<<(unsigned)((nm + 255) / 256), 256, 0, s>>>(h->d_pm_moments, nm, h->d_pm_moments32);
+        e = cudaGetLastError();
+    }
     // the coupling starts at zero like the reference's caches (current_coupling.jl:103-107)
     if (e == cudaSuccess) e = cudaMemsetAsync(h->d_coupling, 0, 8 * c3 * sizeof(double), s);
     if (e == cudaSuccess) e = cudaMemsetAsync(h->d_U, 0, 4 * c3 * sizeof(double), s);
@@ -301,7 +343,7 @@ extern "C" int rpl_update_coupling(rpl_handle* hh) {
     cudaError_t e = cudaSetDevice(h->device);
     if (e != cudaSuccess) return pm_fail(RPL_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
     if (!h->pm) return RPL_OK;  // prescribed currents are static: rpl_set_currents already applied them
-    e = rpl::launch_pm_refresh(*h, h->N, h->stream);
+    e = rpl::launch_pm_refresh(*h, h->N, h->stream, true);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) return pm_fail(RPL_ERR_CUDA, std::string("rpl_update_coupling: ") + cudaGetErrorString(e));
     return RPL_OK;
