@@ -62,6 +62,9 @@ def parse():
     ap.add_argument("--refresh-currents", action="store_true",
                     help="time-varying currents (--workload seamount): new u, v every step, projected again "
                          "(rpl_update_currents_device in the timed region; from pinned host buffers in e2e)")
+    ap.add_argument("--output-every", type=int, default=0,
+                    help="output during the timed steps: diagnostics into a device time series every step and an "
+                         "asynchronous snapshot of the action to pinned host memory every K steps")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
@@ -278,12 +281,31 @@ def run_ours(args, rank, world, local_rank):
         _lib.check(lib.rpl_update_currents_device(h, _lib.ctypes.c_void_p(cur[k % 2][0].data_ptr()),
                                                   _lib.ctypes.c_void_p(cur[k % 2][1].data_ptr())))
 
+    # output: two pinned snapshot buffers used in turn, a device time series of the total action
+    snap_bufs, series = None, None
+    if args.output_every > 0:
+        snap_bufs = [rp.HostBuffer(m.action.size, np.float32 if args.precision == "fp32" else np.float64)
+                     for _ in range(2)]
+        series = torch.zeros(max(args.steps, 1), dtype=torch.float64, device=f"cuda:{local_rank}")
+        torch.cuda.synchronize()
+
+    def output(k):
+        _lib.check(lib.rpl_diagnostics_device(h, None, None, None, None,
+                                              _lib.ctypes.c_void_p(series[k:k + 1].data_ptr())))
+        if (k + 1) % args.output_every == 0:
+            buf = snap_bufs[(k // args.output_every) % 2]
+            _lib.check(lib.rpl_snapshot_async(h, buf.ptr, _lib.RPL_F32 if args.precision == "fp32" else _lib.RPL_F64))
+
     # warm-up
     for k in range(args.warmup):
         if cur is not None:
             refresh(k)
         _lib.check(lib.rpl_step_async(h, dt, 1))
+        if snap_bufs is not None:
+            output(0)
     _lib.check(lib.rpl_sync(h))
+    if snap_bufs is not None:
+        _lib.check(lib.rpl_snapshot_wait(h))
     barrier()
 
     # device-timed region: K steps, events around each stage launch on the launching stream
@@ -302,9 +324,15 @@ def run_ours(args, rank, world, local_rank):
                 for s in (1, 2, 3):
                     _lib.check(lib.rpl_stage_async(h, dt, s))
                     ev[k][s].record(torch_stream)
+                if snap_bufs is not None:
+                    output(k)
             end.record(torch_stream)
         torch_stream.synchronize()
         _lib.check(lib.rpl_sync(h))
+        if snap_bufs is not None:
+            t_wait = time.perf_counter()
+            _lib.check(lib.rpl_snapshot_wait(h))
+            snap_tail_ms = 1e3 * (time.perf_counter() - t_wait)
         barrier()
     ms = start.elapsed_time(end)
     stage_ms = [ev[k][s].elapsed_time(ev[k][s + 1]) for k in range(args.steps) for s in range(3)]
@@ -379,7 +407,12 @@ def run_ours(args, rank, world, local_rank):
                        "l2": "state (%.1f GB per buffer) larger than L2; no flush" % (w.units * (4 if args.precision == "fp32" else 8) / 1e9),
                        "parallelism": f"{world} independent replicas" if world > 1 else "1 GPU",
                        **({"currents": "time-varying: new u, v every step (Q transform + gradients + coefficients "
-                                       "in the timed region)", "currents_refresh_ms": refresh_ms} if cur else {})},
+                                       "in the timed region)", "currents_refresh_ms": refresh_ms} if cur else {}),
+                       **({"output": {"diagnostics": "total action into a device time series every step",
+                                      "snapshot_every": args.output_every,
+                                      "snapshot_bytes": snap_bufs[0].array.nbytes,
+                                      "snapshot_copy_after_timed_region_ms": snap_tail_ms}}
+                          if snap_bufs is not None else {})},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "peak_kind": peak_kind,
                          "kernel": "tile_kernel" if args.precision == "fp32" else "column_kernel",
@@ -388,7 +421,8 @@ def run_ours(args, rank, world, local_rank):
                                                                "selfcoupled": " incl. its coupling refresh"}.get(
                                                                    args.workload, " incl. its wind/stress-cap kernels")},
             "cpu_baseline": cpu, "e2e": e2e,
-            "gpu_launches": (launches_per_step(args.workload) + (3 if cur else 0)) * args.steps,
+            "gpu_launches": (launches_per_step(args.workload) + (3 if cur else 0) + (2 if snap_bufs else 0)) * args.steps
+                            + (args.steps // args.output_every if snap_bufs else 0),
             "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
@@ -521,7 +555,12 @@ def run_ensemble(args, rank, world, local_rank):
                        "l2": "state (%.1f GB per buffer set) larger than L2; no flush" % (4 * units / 1e9),
                        "parallelism": f"{world} independent replicas" if world > 1 else "1 GPU",
                        **({"currents": "time-varying: new u, v every step (Q transform + gradients + coefficients "
-                                       "in the timed region)", "currents_refresh_ms": refresh_ms} if cur else {})},
+                                       "in the timed region)", "currents_refresh_ms": refresh_ms} if cur else {}),
+                       **({"output": {"diagnostics": "total action into a device time series every step",
+                                      "snapshot_every": args.output_every,
+                                      "snapshot_bytes": snap_bufs[0].array.nbytes,
+                                      "snapshot_copy_after_timed_region_ms": snap_tail_ms}}
+                          if snap_bufs is not None else {})},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": None, "peak_kind": peak_kind, "kernel": "ensemble_kernel",
                          "launch_ms": launch_ms, "algorithmic_bytes_per_launch": nbytes_alg / 3.0,

@@ -194,6 +194,26 @@ int rpl_tendency(rpl_handle* h, double* G, int32_t layout);
 int rpl_diagnostics(rpl_handle* h, double* m0, double* hs, double* krms, double* mean_dir,
                     double* total_action);
 
+/* The diagnostics of rpl_diagnostics written to device memory on the handle's device, enqueued on the
+ * handle's stream without waiting (a per-step time series needs no host round trip); any pointer may
+ * be NULL. */
+int rpl_diagnostics_device(rpl_handle* h, double* m0, double* hs, double* krms, double* mean_dir,
+                           double* total_action);
+
+/* Replaces fetch_output(field::ProductField, model) = interior(field) (OceananigansIntegration.jl:7-9)
+ * for output writers: enqueues a copy of the current action, converted to `dtype` in RPL_LAYOUT_XFAST,
+ * into `host` (Nx*Ny*Nk*Np values) and returns at once. The conversion runs on the handle's stream
+ * into a staging buffer in device memory (allocated at the first call; RPL_ERR_OOM beyond the memory
+ * limit); the device-to-host copy runs on a second stream while later steps proceed. `host` must stay
+ * valid until rpl_snapshot_wait; pinned memory (rpl_host_alloc) lets the copy overlap the steps. A new
+ * snapshot waits on the device for the previous copy. */
+int rpl_snapshot_async(rpl_handle* h, void* host, int32_t dtype);
+/* Blocks until the last snapshot has reached the host. */
+int rpl_snapshot_wait(rpl_handle* h);
+/* Page-locked host memory for snapshots and state transfers (cudaHostAlloc / cudaFreeHost). */
+int rpl_host_alloc(int64_t bytes, void** ptr);
+int rpl_host_free(void* ptr);
+
 /* Largest Nx*Ny that rpl_diagnostics_static accepts (2048 x 2048 cells). */
 #define RPL_STATIC_MAX_COLUMNS 4194304
 

@@ -69,6 +69,7 @@ cudaError_t dalloc(Handle* h, T** p, size_t count) {
 }
 
 void free_all(Handle* h) {
+    rpl::free_output(h);
     rpl::free_learned(h);
     rpl::free_pm(h);
     rpl::free_currents(h);

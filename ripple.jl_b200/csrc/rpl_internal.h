@@ -160,6 +160,13 @@ struct Handle {
     std::vector<double> track_t, track_x, track_y;
     double* d_wind = nullptr;      // 4 arrays of (Nx,Ny): U10 theta ustar factor
     bool wind_field_set = false;
+    // snapshot export (rpl_output.cu)
+    cudaStream_t snap_stream = nullptr;  // device-to-host copies of snapshots
+    cudaEvent_t snap_ready = nullptr;    // the staging buffer holds the snapshot
+    cudaEvent_t snap_done = nullptr;     // the staging buffer has reached the host
+    void* d_snap = nullptr;              // staging buffer, caller layout
+    int64_t snap_bytes = 0;
+    bool snap_pending = false;
     // diagnostics scratch
     double* d_diag = nullptr;      // 5 (Nx,Ny) fields + block partials
     unsigned int* d_err = nullptr;
@@ -185,6 +192,8 @@ cudaError_t launch_pm_derivative(const Handle& h, cudaStream_t s);
 void free_pm(Handle* h);
 // Releases the prescribed-currents state of rpl_set_currents (rpl_api.cu).
 void free_currents(Handle* h);
+// Waits for and releases the snapshot stream, events and staging buffer (rpl_output.cu).
+void free_output(Handle* h);
 
 // Sets the thread-local message rpl_last_error() returns (rpl_api.cu).
 void set_last_error(const std::string& msg);

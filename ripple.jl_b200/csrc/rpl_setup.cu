@@ -252,10 +252,25 @@ __device__ __forceinline__ void kadd(double& s, double& c, double v) {
 
 // Per-(i,j) spectral sums (diagnostic_operations.jl:56-165): m0 = sum N w, Hs = 4 sqrt(m0),
 // kappa_rms = sqrt(sum N trace / m0) (0 when m0 = 0), mean direction = atan(sum N mu_y, sum N mu_x).
+// Exact error of s + v folded into the compensation c (Knuth's two-sum: branch-free, and the same error
+// term as the branch form of kadd).
+__device__ __forceinline__ void tadd(double& s, double& c, double v) {
+    const double t = s + v;
+    const double bp = t - s;
+    c += (s - (t - bp)) + (v - bp);
+    s = t;
+}
+
+// Per-(i,j) moments (moments.jl:33-37,100-123): one warp per column, lanes over the kappa rings
+// (coalesced reads of each direction's kappa column); per lane, FP64 sums of blocks of 4 directions
+// folded into compensated totals, then a fixed-order compensated butterfly over the lanes
+// (deterministic). The error stays within a few units in the last place of the sum of |terms|.
 template <typename T>
-__global__ void diag_kernel(const T* __restrict__ N, int64_t Nx, int64_t Ny, int64_t Nk, int64_t Np,
-                            const double* __restrict__ tabs, double* __restrict__ out) {
-    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(256)
+diag_kernel(const T* __restrict__ N, int64_t Nx, int64_t Ny, int64_t Nk, int64_t Np,
+            const double* __restrict__ tabs, double* __restrict__ out) {
+    const int lane = threadIdx.x & 31;
+    const int64_t c = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t P = Nx * Ny;
     if (c >= P) return;
     const int64_t nb = Nk * Np;
@@ -264,18 +279,58 @@ __global__ void diag_kernel(const T* __restrict__ N, int64_t Nx, int64_t Ny, int
     const double* muy = tabs + 2 * nb;
     const double* tr = tabs + 3 * nb;
     double s0 = 0, c0 = 0, sx = 0, cx = 0, sy = 0, cy = 0, st = 0, ct = 0;
-    for (int64_t b = 0; b < nb; ++b) {
-        const double a = (double)N[((b / Nk) * P + c) * Nk + b % Nk];  // bin b = m + Nk*n
-        kadd(s0, c0, a * w[b]);
-        kadd(sx, cx, a * mux[b]);
-        kadd(sy, cy, a * muy[b]);
-        kadd(st, ct, a * tr[b]);
+    const int64_t stride = P * Nk;  // between directions
+    const int nk = (int)Nk, np = (int)Np;
+    for (int m = lane; m < nk; m += 32) {
+        const T* p = N + c * Nk + m;
+        // blocks of DB directions: the block's loads are issued together, its terms summed with FMAs,
+        // and the block sum folded into the compensated totals
+        constexpr int DB = 4;
+        for (int n0 = 0; n0 < np; n0 += DB, p += DB * stride) {
+            double a[DB];
+            int b[DB];
+#pragma unroll
+            for (int k = 0; k < DB; ++k) {
+                const bool in = n0 + k < np;
+                a[k] = in ? (double)p[k * stride] : 0.0;
+                b[k] = in ? m + nk * (n0 + k) : m;  // a[k] = 0 past the last direction
+            }
+            double b0 = 0.0, bx = 0.0, by = 0.0, bt = 0.0;
+#pragma unroll
+            for (int k = 0; k < DB; ++k) {
+                b0 = fma(a[k], __ldg(w + b[k]), b0);
+                bx = fma(a[k], __ldg(mux + b[k]), bx);
+                by = fma(a[k], __ldg(muy + b[k]), by);
+                bt = fma(a[k], __ldg(tr + b[k]), bt);
+            }
+            tadd(s0, c0, b0);
+            tadd(sx, cx, bx);
+            tadd(sy, cy, by);
+            tadd(st, ct, bt);
+        }
     }
-    const double m0 = s0 + c0, mx = sx + cx, my = sy + cy, mt = st + ct;
-    out[c] = m0;
-    out[P + c] = 4.0 * sqrt(m0);
-    out[2 * P + c] = sqrt(m0 == 0.0 ? 0.0 : mt / m0);
-    out[3 * P + c] = atan2(my, mx);
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        double so = __shfl_down_sync(0xffffffffu, s0, off), co = __shfl_down_sync(0xffffffffu, c0, off);
+        tadd(s0, c0, so);
+        c0 += co;
+        so = __shfl_down_sync(0xffffffffu, sx, off), co = __shfl_down_sync(0xffffffffu, cx, off);
+        tadd(sx, cx, so);
+        cx += co;
+        so = __shfl_down_sync(0xffffffffu, sy, off), co = __shfl_down_sync(0xffffffffu, cy, off);
+        tadd(sy, cy, so);
+        cy += co;
+        so = __shfl_down_sync(0xffffffffu, st, off), co = __shfl_down_sync(0xffffffffu, ct, off);
+        tadd(st, ct, so);
+        ct += co;
+    }
+    if (lane == 0) {
+        const double m0 = s0 + c0, mx = sx + cx, my = sy + cy, mt = st + ct;
+        out[c] = m0;
+        out[P + c] = 4.0 * sqrt(m0);
+        out[2 * P + c] = sqrt(m0 == 0.0 ? 0.0 : mt / m0);
+        out[3 * P + c] = atan2(my, mx);
+    }
 }
 
 // Total action = sum_ij m0 dx dy with a compensated, deterministic two-level reduction.
@@ -471,11 +526,11 @@ cudaError_t launch_diagnostics(const Handle& h, const void* Nin, cudaStream_t s)
     const rpl_desc& d = h.desc;
     const int64_t P = d.Nx * d.Ny;
     if (h.precision == RPL_FP64)
-        diag_kernel<double><<<blocks_for(P, 128), 128, 0, s>>>((const double*)Nin, d.Nx, d.Ny, d.Nk, d.Np,
-                                                               h.d_weights, h.d_diag);
+        diag_kernel<double><<<blocks_for(P * 32, 256), 256, 0, s>>>((const double*)Nin, d.Nx, d.Ny, d.Nk, d.Np,
+                                                                    h.d_weights, h.d_diag);
     else
-        diag_kernel<float><<<blocks_for(P, 128), 128, 0, s>>>((const float*)Nin, d.Nx, d.Ny, d.Nk, d.Np,
-                                                              h.d_weights, h.d_diag);
+        diag_kernel<float><<<blocks_for(P * 32, 256), 256, 0, s>>>((const float*)Nin, d.Nx, d.Ny, d.Nk, d.Np,
+                                                                   h.d_weights, h.d_diag);
     total_kernel<<<1, 1024, 0, s>>>(h.d_diag, P, d.dx * d.dy, h.d_diag + 4 * P);
     return cudaGetLastError();
 }

@@ -12,6 +12,8 @@ from .sources import (BulkWindDrag, Clockwise, Counterclockwise, HollandHurrican
 from .model import (Clock, ProductField, PseudomomentumVelocities, Simulation, SpectralWaveModel, WENO, WaveActionField,
                     compute_tendencies, interior, run_, set_, time_step, update_coupling)
 from .ensemble import Ensemble
+from .output import (HostBuffer, SnapshotWriter, diagnostics_device, fetch_output, snapshot_async,
+                     snapshot_wait)
 from . import learned
 from .diagnostics import (diagnostics, m0, mean_direction, mean_period, root_mean_square_wavenumber,
                           significant_wave_height, total_action)

@@ -84,6 +84,11 @@ _SIGNATURES = {
     "rpl_set_currents": (ctypes.c_int, [ctypes.c_void_p, _i64, _dp, _i32, _d, _dp, _dp, _dp, _d]),
     "rpl_get_coupling": (ctypes.c_int, [ctypes.c_void_p] + [_dp] * 8),
     "rpl_update_currents": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp]),
+    "rpl_diagnostics_device": (ctypes.c_int, [ctypes.c_void_p] + [ctypes.c_void_p] * 5),
+    "rpl_snapshot_async": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, _i32]),
+    "rpl_snapshot_wait": (ctypes.c_int, [ctypes.c_void_p]),
+    "rpl_host_alloc": (ctypes.c_int, [_i64, ctypes.POINTER(ctypes.c_void_p)]),
+    "rpl_host_free": (ctypes.c_int, [ctypes.c_void_p]),
     "rpl_update_currents_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "rpl_set_pseudomomentum": (ctypes.c_int, [ctypes.c_void_p, _i64, _dp, _i32, _d, _dp, _d]),
     "rpl_update_coupling": (ctypes.c_int, [ctypes.c_void_p]),
