@@ -65,6 +65,8 @@ def parse():
     ap.add_argument("--output-every", type=int, default=0,
                     help="output during the timed steps: diagnostics into a device time series every step and an "
                          "asynchronous snapshot of the action to pinned host memory every K steps")
+    ap.add_argument("--smoothing", action="store_true",
+                    help="propagation_smoothing = SpatialAveraging() after every step (the reference's hurricane example)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
@@ -251,6 +253,8 @@ def run_ours(args, rank, world, local_rank):
         smi_id = str(local_rank)
     w = make_workload(args.workload, args.size, args.steps,
                       n0_dtype=np.float32 if args.precision == "fp32" else np.float64)
+    if args.smoothing:
+        w.propagation_smoothing = rp.SpatialAveraging()
     m = w.model(args.precision, device=local_rank)
     lib, h = m._lib, m.handle
     torch_stream = torch.cuda.Stream(device=local_rank)
@@ -408,6 +412,8 @@ def run_ours(args, rank, world, local_rank):
                        "parallelism": f"{world} independent replicas" if world > 1 else "1 GPU",
                        **({"currents": "time-varying: new u, v every step (Q transform + gradients + coefficients "
                                        "in the timed region)", "currents_refresh_ms": refresh_ms} if cur else {}),
+                       **({"propagation_smoothing": "SpatialAveraging(αs=0.5, αn=0.5) after every step"}
+                          if args.smoothing else {}),
                        **({"output": {"diagnostics": "total action into a device time series every step",
                                       "snapshot_every": args.output_every,
                                       "snapshot_bytes": snap_bufs[0].array.nbytes,
@@ -421,7 +427,8 @@ def run_ours(args, rank, world, local_rank):
                                                                "selfcoupled": " incl. its coupling refresh"}.get(
                                                                    args.workload, " incl. its wind/stress-cap kernels")},
             "cpu_baseline": cpu, "e2e": e2e,
-            "gpu_launches": (launches_per_step(args.workload) + (3 if cur else 0) + (2 if snap_bufs else 0)) * args.steps
+            "gpu_launches": (launches_per_step(args.workload) + (3 if cur else 0) + (2 if snap_bufs else 0)
+                             + (1 if args.smoothing else 0)) * args.steps
                             + (args.steps // args.output_every if snap_bufs else 0),
             "clocks": clocks,
         }
@@ -556,6 +563,8 @@ def run_ensemble(args, rank, world, local_rank):
                        "parallelism": f"{world} independent replicas" if world > 1 else "1 GPU",
                        **({"currents": "time-varying: new u, v every step (Q transform + gradients + coefficients "
                                        "in the timed region)", "currents_refresh_ms": refresh_ms} if cur else {}),
+                       **({"propagation_smoothing": "SpatialAveraging(αs=0.5, αn=0.5) after every step"}
+                          if args.smoothing else {}),
                        **({"output": {"diagnostics": "total action into a device time series every step",
                                       "snapshot_every": args.output_every,
                                       "snapshot_bytes": snap_bufs[0].array.nbytes,

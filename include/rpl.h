@@ -155,6 +155,12 @@ int rpl_update_coupling(rpl_handle* h);
 int rpl_get_coupling(rpl_handle* h, double* Ux, double* Uy, double* dUxdk, double* dUydk,
                      double* Uxx, double* Uxy, double* Uyx, double* Uyy);
 
+/* Replaces SpectralWaveModel(...; propagation_smoothing=SpatialAveraging(; αs, αn)) and
+ * apply_propagation_smoothing! after every step (propagation_smoothing.jl:20-199, time_step.jl:168):
+ * kind 1 = SpatialAveraging (Tolman 2002 GSE alleviation), 0 = none. The averaging runs on the device
+ * after each RK3 step, in the state's precision with FP64 corner positions. */
+int rpl_set_propagation_smoothing(rpl_handle* h, int32_t kind, double alpha_s, double alpha_n);
+
 /* Replaces the sources kwarg + prepare_sources (precomputed_sources.jl:386-394). */
 int rpl_set_sources(rpl_handle* h, const rpl_sources* s);
 /* Host-evaluated wind (any wind struct of src/Forcing/winds.jl) for RPL_WIND_FIELD: (Nx,Ny) arrays. */

@@ -39,7 +39,8 @@ class OraModel(ctypes.Structure):
                 ("z_alpha", _d), ("p_in", _d), ("alpha0", _d), ("rho_air", _d), ("rho_water", _d),
                 ("von_karman", _d), ("gravity", _d), ("has_dissipation", _i32), ("C_ds", _d), ("B_r", _d),
                 ("ds_p", _d), ("sigma_power", _d), ("ds_gravity", _d), ("pm_mode", _i32), ("pm_per_cell", _i32),
-                ("pm_overlap", _dp), ("pm_kx", _dp), ("pm_ky", _dp)]
+                ("pm_overlap", _dp), ("pm_kx", _dp), ("pm_ky", _dp), ("gse", _i32), ("periodic_x", _i32),
+                ("periodic_y", _i32), ("gse_alpha_s", _d), ("gse_alpha_n", _d)]
 
 
 def build():
@@ -85,6 +86,7 @@ def lib():
                                               _dp, _dp, _dp, _dp]
         L.ora_pm_cells.argtypes = [_i64, _i64, _i64, _i64, _dp, _i64, _dp, _dp, _d, _dp, _dp, _dp, _d, _i32,
                                    _dp, _dp]
+        L.ora_spatial_averaging.argtypes = [ctypes.POINTER(OraModel), _dp, _d]
         L.ora_num_threads.restype = ctypes.c_int
         L.ora_set_num_threads.argtypes = [ctypes.c_int]
         _lib = L
@@ -194,6 +196,11 @@ class Oracle:
         else:
             m.transport = TRANSPORT_NONE
         self._set_sources(w.sources)
+        m.periodic_x = int(g.topology[0] == "Periodic")
+        m.periodic_y = int(g.topology[1] == "Periodic")
+        ps = getattr(w, "propagation_smoothing", None)
+        if ps is not None:
+            m.gse, m.gse_alpha_s, m.gse_alpha_n = 1, float(ps.αs), float(ps.αn)
 
     def _set_currents(self, w, u=None, v=None):
         L = lib()
@@ -355,6 +362,12 @@ class Oracle:
         tt = np.array([float(t)])
         lib().ora_rk3_step(ctypes.byref(self.m), p(N), float(dt), int(nsteps), p(tt))
         return N, float(tt[0])
+
+    def spatial_averaging(self, N, dt):
+        """SpatialAveraging applied once (propagation_smoothing.jl:60-199)."""
+        N = xfast(N).copy(order="F")
+        lib().ora_spatial_averaging(ctypes.byref(self.m), p(N), float(dt))
+        return N
 
     def stress_factor(self, N, t=0.0):
         out = np.empty((self.Nx, self.Ny), order="F")

@@ -698,6 +698,62 @@ void ora_tendency(const ora_model* M, const double* N, double t, int32_t with_so
     if (with_sources && (M->wind_kind != ORA_WIND_NONE || M->has_dissipation)) add_sources(M, N, t, G);
 }
 
+/* src/Models/propagation_smoothing.jl:60-109 (_spatial_averaging_kernel!), :117-158 (tables),
+ * :163-199 (apply). Index arithmetic is 1-based like the reference so the bilinear weights round the
+ * same way; a corner that one periodic wrap does not bring into range is clamped (the reference would
+ * read its halo there; with a CFL-limited dt the corners stay within one cell). */
+void ora_spatial_averaging(const ora_model* M, double* N, double dt) {
+    const int64_t Nx = M->Nx, Ny = M->Ny, Nk = M->Nk, Np = M->Np, P = Nx * Ny;
+    const double g = 9.81;
+    std::vector<double> cg(Nk), dcg(Nk), cs(Np), sn(Np);
+    for (int64_t m = 0; m < Nk; ++m) cg[m] = 1.0 / 2.0 * std::sqrt(g / M->kappa[m]);
+    for (int64_t m = 0; m < Nk; ++m) {
+        const double lo = m == 0 ? cg[0] : 1.0 / 2.0 * std::sqrt(g / M->kappa[m - 1]);
+        const double hi = m == Nk - 1 ? cg[Nk - 1] : 1.0 / 2.0 * std::sqrt(g / M->kappa[m + 1]);
+        dcg[m] = std::fabs(lo - hi) / 2.0;
+    }
+    for (int64_t n = 0; n < Np; ++n) {
+        cs[n] = std::cos(M->phi[n]);
+        sn[n] = std::sin(M->phi[n]);
+    }
+    const double dphi = M->phi_faces[1] - M->phi_faces[0];
+    const double dx_inv = 1.0 / M->dx, dy_inv = 1.0 / M->dy;
+    const double as = M->gse_alpha_s, an = M->gse_alpha_n;
+    auto wrap = [](int64_t i, int64_t n, int32_t periodic) {
+        if (periodic) i = i < 1 ? i + n : (i > n ? i - n : i);
+        return i < 1 ? (int64_t)1 : (i > n ? n : i);
+    };
+    std::vector<double> out((size_t)(P * Nk * Np));
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int64_t n = 0; n < Np; ++n)
+        for (int64_t m = 0; m < Nk; ++m) {
+            const double Ls = as * dcg[m] * dt, Ln = an * cg[m] * dphi * dt;
+            const double Ls_x = Ls * cs[n] * dx_inv, Ls_y = Ls * sn[n] * dy_inv;
+            const double Ln_x = -Ln * sn[n] * dx_inv, Ln_y = Ln * cs[n] * dy_inv;
+            const double* plane = N + P * (m + Nk * n);
+            for (int64_t j = 1; j <= Ny; ++j)
+                for (int64_t i = 1; i <= Nx; ++i) {
+                    double acc = 0.0;
+                    for (int s1 = -1; s1 <= 1; s1 += 2)
+                        for (int s2 = -1; s2 <= 1; s2 += 2) {
+                            const double di = s1 * Ls_x + s2 * Ln_x, dj = s1 * Ls_y + s2 * Ln_y;
+                            const double ir = (double)i + di, jr = (double)j + dj;
+                            const double fi = std::floor(ir), fj = std::floor(jr);
+                            const int64_t i0 = (int64_t)fi, j0 = (int64_t)fj;
+                            const double wi = ir - (double)i0, wj = jr - (double)j0;
+                            const int64_t i0c = wrap(i0, Nx, M->periodic_x), i1c = wrap(i0 + 1, Nx, M->periodic_x);
+                            const int64_t j0c = wrap(j0, Ny, M->periodic_y), j1c = wrap(j0 + 1, Ny, M->periodic_y);
+                            const double f00 = plane[(i0c - 1) + Nx * (j0c - 1)], f10 = plane[(i1c - 1) + Nx * (j0c - 1)];
+                            const double f01 = plane[(i0c - 1) + Nx * (j1c - 1)], f11 = plane[(i1c - 1) + Nx * (j1c - 1)];
+                            acc += (1.0 - wi) * (1.0 - wj) * f00 + wi * (1.0 - wj) * f10 + (1.0 - wi) * wj * f01 +
+                                   wi * wj * f11;
+                        }
+                    out[(size_t)((i - 1) + Nx * (j - 1) + P * (m + Nk * n))] = acc / 4.0;
+                }
+        }
+    std::memcpy(N, out.data(), sizeof(double) * out.size());
+}
+
 /* src/Models/time_step.jl:138-152,168 (SSP-RK3 with max(0,.) after every stage kernel) */
 void ora_rk3_step(const ora_model* M, double* N, double dt, int64_t nsteps, double* t) {
     const int64_t total = M->Nx * M->Ny * M->Nk * M->Np;
@@ -720,6 +776,7 @@ void ora_rk3_step(const ora_model* M, double* N, double dt, int64_t nsteps, doub
             const double stage = relu(N[u] + dt * G[u]);
             N[u] = relu(a3 * N0[u] + b3 * stage);
         }
+        if (M->gse) ora_spatial_averaging(M, N, dt);  /* time_step.jl:168 */
         *t += dt;
     }
 }

@@ -71,6 +71,11 @@ typedef struct ora_model {
     const double* pm_overlap;            /* ora_pm_overlap_tables layout */
     const double* pm_kx;                 /* (Nk,Np) first-moment measures */
     const double* pm_ky;
+    /* propagation_smoothing = SpatialAveraging(alpha_s, alpha_n) after every RK3 step
+     * (propagation_smoothing.jl:20-199, time_step.jl:168) */
+    int32_t gse;
+    int32_t periodic_x, periodic_y;
+    double gse_alpha_s, gse_alpha_n;
 } ora_model;
 
 /* ---- Q kernel (src/Coupling/q_kernel.jl) ---- */
@@ -127,6 +132,8 @@ void ora_wind_fields(const ora_model* M, double t, double* U10, double* theta, d
 void ora_tendency(const ora_model* M, const double* N, double t, int32_t with_sources, double* G);
 void ora_stress_factor(const ora_model* M, const double* N, double t, double* factor);
 void ora_rk3_step(const ora_model* M, double* N, double dt, int64_t nsteps, double* t);
+/* SpatialAveraging applied once to N (x fastest) with the step's dt (propagation_smoothing.jl:60-199). */
+void ora_spatial_averaging(const ora_model* M, double* N, double dt);
 
 /* ---- diagnostics (src/Diagnostics) ---- */
 void ora_diagnostics(const ora_model* M, const double* N,

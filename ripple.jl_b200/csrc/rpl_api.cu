@@ -70,6 +70,7 @@ cudaError_t dalloc(Handle* h, T** p, size_t count) {
 
 void free_all(Handle* h) {
     rpl::free_output(h);
+    rpl::free_smooth(h);
     rpl::free_learned(h);
     rpl::free_pm(h);
     rpl::free_currents(h);
@@ -143,7 +144,8 @@ int launch_step(Handle* h, double dt, int stage_only) {
     const int first = stage_only ? stage_only : 1, last = stage_only ? stage_only : 3;
     for (int stage = first; stage <= last; ++stage) {
         const void* Nin = stage == 1 ? h->N : (stage == 2 ? h->A : h->B);
-        void* Nout = stage == 1 ? h->A : (stage == 2 ? h->B : h->N);
+        // with SpatialAveraging, stage 3 writes into A (free by then) and the averaging writes A -> N
+        void* Nout = stage == 1 ? h->A : (stage == 2 ? h->B : (h->smooth ? h->A : h->N));
         if (sources) {
             if (stage == 1) RPL_CUDA(rpl::launch_wind(*h, h->time, s));
             if (h->learned) RPL_CUDA(rpl::launch_learned_stage_prep(*h, Nin, s));
@@ -152,6 +154,7 @@ int launch_step(Handle* h, double dt, int stage_only) {
         if (h->pm) RPL_CUDA(rpl::launch_pm_refresh(*h, Nin, s, false));
         const rpl::StageParams p = rpl::make_params(*h, dt, stage);
         RPL_CUDA(rpl::launch_stage(*h, p, Nin, h->N, Nout, s));
+        if (stage == 3 && h->smooth) RPL_CUDA(rpl::launch_smooth(*h, h->A, h->N, dt, s));  // time_step.jl:168
     }
     if (last == 3) {
         h->time += dt;

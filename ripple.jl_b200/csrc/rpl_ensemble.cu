@@ -343,6 +343,7 @@ int rpl_ensemble_create(rpl_handle* const* members, const double* dt, int32_t co
             return efail(RPL_ERR_STATE, who + "refraction transport needs rpl_set_currents first");
         if (h.pm)
             return efail(RPL_ERR_UNSUPPORTED, who + "ensemble members take prescribed currents, not pseudomomentum");
+        if (h.smooth) return efail(RPL_ERR_UNSUPPORTED, who + "ensemble members carry no propagation smoothing");
     }
     cudaError_t err = cudaSetDevice(h0.device);
     if (err != cudaSuccess) return ecuda(err, "cudaSetDevice");

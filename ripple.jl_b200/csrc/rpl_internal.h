@@ -160,6 +160,11 @@ struct Handle {
     std::vector<double> track_t, track_x, track_y;
     double* d_wind = nullptr;      // 4 arrays of (Nx,Ny): U10 theta ustar factor
     bool wind_field_set = false;
+    // propagation_smoothing = SpatialAveraging (rpl_smooth.cu)
+    bool smooth = false;
+    double smooth_as = 0.5, smooth_an = 0.5, smooth_dt = -1.0;  // dt of the current per-bin stencils
+    void* d_smooth = nullptr;      // FP64 cg[Nk], dcg[Nk], cos[Np], sin[Np]; per-bin 3x3 stencils; far flags
+    int64_t smooth_bytes = 0;
     // snapshot export (rpl_output.cu)
     cudaStream_t snap_stream = nullptr;  // device-to-host copies of snapshots
     cudaEvent_t snap_ready = nullptr;    // the staging buffer holds the snapshot
@@ -194,6 +199,9 @@ void free_pm(Handle* h);
 void free_currents(Handle* h);
 // Waits for and releases the snapshot stream, events and staging buffer (rpl_output.cu).
 void free_output(Handle* h);
+// SpatialAveraging of the state Nin into Nout with the step's dt; release of its tables (rpl_smooth.cu).
+cudaError_t launch_smooth(Handle& h, const void* Nin, void* Nout, double dt, cudaStream_t s);
+void free_smooth(Handle* h);
 
 // Sets the thread-local message rpl_last_error() returns (rpl_api.cu).
 void set_last_error(const std::string& msg);

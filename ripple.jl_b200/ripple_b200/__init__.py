@@ -9,7 +9,7 @@ from .grids import (Bounded, Flat, InfiniteDepth, Periodic, PolarWaveVectorGrid,
                     centers_to_faces, lower_bounded_centers_to_faces)
 from .sources import (BulkWindDrag, Clockwise, Counterclockwise, HollandHurricaneWind, LinearStormTrack,
                       LocalSaturationDissipation, PrecomputedSources, PressureCorrelationInput)
-from .model import (Clock, ProductField, PseudomomentumVelocities, Simulation, SpectralWaveModel, WENO, WaveActionField,
+from .model import (Clock, ProductField, PseudomomentumVelocities, Simulation, SpatialAveraging, SpectralWaveModel, WENO, WaveActionField,
                     compute_tendencies, interior, run_, set_, time_step, update_coupling)
 from .ensemble import Ensemble
 from .output import (HostBuffer, SnapshotWriter, diagnostics_device, fetch_output, snapshot_async,

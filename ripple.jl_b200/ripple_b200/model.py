@@ -37,6 +37,19 @@ class Clock:
 _UNSET = object()
 
 
+class SpatialAveraging:
+    """Tolman (2002) spatial-averaging GSE alleviation applied after every time step
+    (propagation_smoothing.jl:20-56): each bin's field is replaced by the mean of four bilinear samples
+    at the corners of a rectangle of half-widths αs·|Δc_g|·Δt along and αn·c_g·Δφ·Δt across its
+    propagation direction."""
+
+    def __init__(self, *, αs=0.5, αn=0.5, alpha_s=None, alpha_n=None):
+        self.αs = float(alpha_s if alpha_s is not None else αs)
+        self.αn = float(alpha_n if alpha_n is not None else αn)
+        if not (self.αs >= 0 and self.αn >= 0 and math.isfinite(self.αs) and math.isfinite(self.αn)):
+            raise ArgumentError("SpatialAveraging needs finite αs, αn >= 0")
+
+
 class PseudomomentumVelocities:
     """uᴸ = p: the waves' own pseudomomentum drives their Doppler shift (lagrangian_velocities.jl:55-81).
     The coupling is recomputed from the action before every RK3 stage. Without `q_grid` a Flat wave grid
@@ -191,8 +204,8 @@ class SpectralWaveModel:
             raise ArgumentError("spectral_grid must be a PolarWaveVectorGrid on this path")
         if coupling is not None:
             raise ArgumentError("pass `velocities`; prebuilt couplings are not supported")
-        if propagation_smoothing is not None:
-            raise ArgumentError("propagation_smoothing is outside this path")
+        if propagation_smoothing is not None and not isinstance(propagation_smoothing, SpatialAveraging):
+            raise ArgumentError("propagation_smoothing must be nothing or SpatialAveraging()")
         ts = str(timestepper).lstrip(":")
         if ts != "RK3":
             raise ArgumentError(f"unsupported timestepper {timestepper} (the B200 path implements :RK3)")
@@ -215,6 +228,7 @@ class SpectralWaveModel:
         self.spectral_advection = spectral_advection
         self.sources = sources
         self.velocities = velocities
+        self.propagation_smoothing = propagation_smoothing
         self.timestepper = "RK3"
         self.precision = precision
         self.device = device
@@ -286,6 +300,8 @@ class SpectralWaveModel:
 
         if velocities is not None:
             self._set_velocities(velocities)
+        if propagation_smoothing is not None:
+            check(lib.rpl_set_propagation_smoothing(h, 1, propagation_smoothing.αs, propagation_smoothing.αn))
         self._field_wind = None
         if sources is not None:
             self._set_sources(sources)

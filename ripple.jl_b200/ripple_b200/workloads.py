@@ -41,6 +41,7 @@ class Workload:
     sources: object = None
     horizontal_advection: object = field(default_factory=WENO)
     notes: dict = field(default_factory=dict)
+    propagation_smoothing: object = None
 
     @property
     def units(self):
@@ -49,6 +50,7 @@ class Workload:
     def model(self, precision="fp64", **kw):
         m = SpectralWaveModel(self.grid, self.spectral_grid, depth=self.depth, velocities=self.velocities,
                               sources=self.sources, horizontal_advection=self.horizontal_advection,
+                              propagation_smoothing=self.propagation_smoothing,
                               timestepper="RK3", precision=precision, **kw)
         m.action.set(self.N0)
         return m
