@@ -206,6 +206,15 @@ int rpl_diagnostics(rpl_handle* h, double* m0, double* hs, double* krms, double*
 int rpl_diagnostics_device(rpl_handle* h, double* m0, double* hs, double* krms, double* mean_dir,
                            double* total_action);
 
+/* Row copies for a y-slab domain decomposition (no counterpart in the reference, which runs one domain
+ * per architecture). which: 0 = N (the step's state, input of stage 1), 1 = A (input of stage 2),
+ * 2 = B (input of stage 3). Rows row0 .. row0+nrows-1 of every direction move between the state buffer
+ * and a packed device buffer of (Np, nrows, Nx, Nk) words of the state's type (kappa fastest),
+ * stream-ordered on the handle's stream without waiting. A decomposed step copies each slab's
+ * boundary rows out, exchanges them, copies them into the halo rows, then runs rpl_stage_async. */
+int rpl_rows_get(rpl_handle* h, int32_t which, int64_t row0, int64_t nrows, void* dst);
+int rpl_rows_set(rpl_handle* h, int32_t which, int64_t row0, int64_t nrows, const void* src);
+
 /* Replaces fetch_output(field::ProductField, model) = interior(field) (OceananigansIntegration.jl:7-9)
  * for output writers: enqueues a copy of the current action, converted to `dtype` in RPL_LAYOUT_XFAST,
  * into `host` (Nx*Ny*Nk*Np values) and returns at once. The conversion runs on the handle's stream

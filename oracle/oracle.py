@@ -160,7 +160,8 @@ class Oracle:
         self._x, self._y = f64(g.xnodes()), f64(g.ynodes())
         m = self.m = OraModel()
         m.Nx, m.Ny, m.Nk, m.Np = self.Nx, self.Ny, self.Nk, self.Np
-        m.dx, m.dy = float(g.xspacings()[0]), float(g.yspacings()[0])
+        m.dx, m.dy = g.first_spacings() if hasattr(g, "first_spacings") else (float(g.xspacings()[0]),
+                                                                              float(g.yspacings()[0]))
         m.xnodes, m.ynodes = p(self._x), p(self._y)
         m.kappa, m.kappa_faces, m.phi, m.phi_faces, m.weights = p(k), p(self._kf), p(ph), p(self._pf), p(self._w)
         depth = w.depth

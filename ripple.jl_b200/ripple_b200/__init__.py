@@ -12,6 +12,7 @@ from .sources import (BulkWindDrag, Clockwise, Counterclockwise, HollandHurrican
 from .model import (Clock, ProductField, PseudomomentumVelocities, Simulation, SpatialAveraging, SpectralWaveModel, WENO, WaveActionField,
                     compute_tendencies, interior, run_, set_, time_step, update_coupling)
 from .ensemble import Ensemble
+from . import decomposition
 from .output import (HostBuffer, SnapshotWriter, diagnostics_device, fetch_output, snapshot_async,
                      snapshot_wait)
 from . import learned

@@ -84,6 +84,8 @@ _SIGNATURES = {
     "rpl_set_currents": (ctypes.c_int, [ctypes.c_void_p, _i64, _dp, _i32, _d, _dp, _dp, _dp, _d]),
     "rpl_get_coupling": (ctypes.c_int, [ctypes.c_void_p] + [_dp] * 8),
     "rpl_update_currents": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp]),
+    "rpl_rows_get": (ctypes.c_int, [ctypes.c_void_p, _i32, _i64, _i64, ctypes.c_void_p]),
+    "rpl_rows_set": (ctypes.c_int, [ctypes.c_void_p, _i32, _i64, _i64, ctypes.c_void_p]),
     "rpl_set_propagation_smoothing": (ctypes.c_int, [ctypes.c_void_p, _i32, _d, _d]),
     "rpl_diagnostics_device": (ctypes.c_int, [ctypes.c_void_p] + [ctypes.c_void_p] * 5),
     "rpl_snapshot_async": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, _i32]),

@@ -1,0 +1,229 @@
+"""Y-slab domain decomposition of the SSP-RK3 step across ranks, one GPU each, for domains larger than
+one GPU's memory. The reference runs one domain per architecture; this module has no counterpart there.
+
+Rank r owns rows [start, stop) of the global grid and keeps HALO = 3 rows on either side (the reach of
+the WENO5 stencils in y: the update of row j reads rows j-3 .. j+3). Its local model is an ordinary
+periodic model on stop - start + 6 rows: the stage kernels wrap around at the local array's edges,
+which only corrupts halo rows, and every stage's input has its halo rows refreshed from the neighbouring
+slabs (periodic in y) before the stage runs. Everything else on the path is column- or cell-local
+(Q transform, stress cap, wind, coefficient records; the current gradients at the interior rows read
+halo rows only), so the owned rows evolve exactly as in the undecomposed model: the interior faces,
+nodes and spacings are the parent grid's own values, and the arithmetic per cell is the same.
+
+The exchange per stage: rows are copied out of the stage's input buffer into packed device buffers
+(rpl_rows_get), sent upward then downward with torch.distributed point-to-point operations (NCCL between
+GPUs; gloo between CPU processes in the tests), and copied into the halo rows (rpl_rows_set).
+Pseudomomentum coupling and SpatialAveraging are not decomposed (the averaging would need a halo
+exchange between stage 3 and the averaging).
+"""
+import numpy as np
+
+from ._lib import ArgumentError, check
+from . import _lib
+from .grids import RectilinearGrid
+from .workloads import Workload
+
+HALO = 3
+
+
+def slab_rows(Ny, world, rank):
+    """Rows [start, stop) of rank `rank` in a balanced split of Ny rows."""
+    return rank * Ny // world, (rank + 1) * Ny // world
+
+
+class Slab:
+    """Row bookkeeping of one rank: owned rows, local (halo-extended) rows, neighbours."""
+
+    def __init__(self, Ny, world, rank, halo=HALO):
+        if not 0 <= rank < world:
+            raise ArgumentError("rank out of range")
+        self.Ny, self.world, self.rank, self.halo = Ny, world, rank, halo
+        self.start, self.stop = slab_rows(Ny, world, rank)
+        self.ny = self.stop - self.start
+        if self.ny < halo:
+            raise ArgumentError(f"each rank needs at least {halo} rows (Ny = {Ny}, {world} ranks)")
+        self.rows = self.ny + 2 * halo
+        self.prev, self.next = (rank - 1) % world, (rank + 1) % world
+
+    def global_rows(self):
+        """Global row index (periodic) of every local row."""
+        return np.arange(self.start - self.halo, self.stop + self.halo) % self.Ny
+
+    # local row ranges: (first, count)
+    def send_low(self):
+        return self.halo, self.halo                  # lowest owned rows -> the previous rank's top halo
+
+    def send_high(self):
+        return self.ny, self.halo                    # highest owned rows -> the next rank's bottom halo
+
+    def halo_low(self):
+        return 0, self.halo
+
+    def halo_high(self):
+        return self.halo + self.ny, self.halo
+
+    def owned(self):
+        return slice(self.halo, self.halo + self.ny)
+
+
+def _local_grid(grid, slab):
+    """The slab's grid: the parent's x faces, y faces a + k d of the parent's uniform y axis extended past
+    its ends (so interior faces are the parent's own values), the parent's spacings and z."""
+    yf = grid.yfaces()
+    Ny = grid.Ny
+    d = (yf[-1] - yf[0]) / Ny
+    if not np.allclose(np.diff(yf), d, rtol=1e-12, atol=0.0):
+        raise ArgumentError("the decomposition needs a uniform y axis")
+    k = np.arange(slab.start - slab.halo, slab.stop + slab.halo + 1)
+    inside = (k >= 0) & (k <= Ny)
+    faces = np.where(inside, yf[np.clip(k, 0, Ny)], yf[0] + k * d)
+    size = (grid.Nx, slab.rows) if grid.Nz == 0 else (grid.Nx, slab.rows, grid.Nz)
+    kw = dict(size=size, x=grid.xfaces(), y=faces, topology=(grid.topology[0], "Periodic", grid.topology[2]),
+              first_spacings=grid.first_spacings())
+    if grid.Nz:
+        kw["z"] = grid.zfaces()
+    return RectilinearGrid(**kw)
+
+
+def local_workload(w, slab):
+    """The slab's part of workload `w` (N0, depth, currents on the halo-extended rows)."""
+    g = w.grid
+    if g.topology[1] != "Periodic":
+        raise ArgumentError("the y-slab decomposition needs a periodic y axis")
+    if w.propagation_smoothing is not None:
+        raise ArgumentError("SpatialAveraging is not decomposed")
+    if w.velocities is not None and not isinstance(w.velocities, dict):
+        raise ArgumentError("only prescribed currents are decomposed")
+    rows = slab.global_rows()
+    grid = _local_grid(g, slab)
+    N0 = np.asfortranarray(np.take(w.N0, rows, axis=1))
+    depth = w.depth
+    if not np.isscalar(depth) and type(depth).__name__ != "InfiniteDepth":
+        depth = np.asfortranarray(np.take(np.asarray(depth), rows, axis=1))
+    vel = None
+    if w.velocities is not None:
+        vel = {k: (np.asfortranarray(np.take(np.asarray(v), rows, axis=1)) if k in ("u", "v") else v)
+               for k, v in w.velocities.items()}
+        if "q_grid" in vel:
+            raise ArgumentError("give the currents on the wave grid's own vertical grid")
+    return Workload(f"{w.name}[rows {slab.start}:{slab.stop}]", grid, w.spectral_grid, depth, N0, w.dt, w.nsteps,
+                    velocities=vel, sources=w.sources, horizontal_advection=w.horizontal_advection,
+                    notes=dict(w.notes, slab=(slab.start, slab.stop)))
+
+
+class LibBackend:
+    """The slab's model in librpl.so: row copies and single stages on the handle's stream."""
+
+    def __init__(self, model):
+        self.model = model
+        self.lib, self.h = model._lib, model.handle
+
+    def rows_get(self, which, first, count, buf):
+        check(self.lib.rpl_rows_get(self.h, which, first, count, _lib.ctypes.c_void_p(buf.data_ptr())))
+
+    def rows_set(self, which, first, count, buf):
+        check(self.lib.rpl_rows_set(self.h, which, first, count, _lib.ctypes.c_void_p(buf.data_ptr())))
+
+    def stage(self, dt, s):
+        check(self.lib.rpl_stage_async(self.h, float(dt), int(s)))
+
+    def sync(self):
+        check(self.lib.rpl_sync(self.h))
+        self.model._sync_clock()
+
+
+def _buffers(slab, Nx, Nk, Np, dtype, device):
+    import torch
+    n = Np * slab.halo * Nx * Nk
+    return {k: torch.empty(n, dtype=dtype, device=device) for k in ("send_low", "send_high", "recv_low", "recv_high")}
+
+
+def exchange_dist(backend, slab, which, bufs, group=None):
+    """Refresh the halo rows of buffer `which` from the neighbouring ranks: owned high rows go up to the
+    next rank's bottom halo, then owned low rows go down to the previous rank's top halo. Each phase is
+    one send and one receive per rank, so ranks that are each other's previous and next (two ranks) pair
+    their messages unambiguously."""
+    import torch.distributed as dist
+    backend.rows_get(which, *slab.send_low(), bufs["send_low"])
+    backend.rows_get(which, *slab.send_high(), bufs["send_high"])
+    if slab.world == 1:
+        bufs["recv_low"].copy_(bufs["send_high"])
+        bufs["recv_high"].copy_(bufs["send_low"])
+    else:
+        for send, dst, recv, src in ((bufs["send_high"], slab.next, bufs["recv_low"], slab.prev),
+                                     (bufs["send_low"], slab.prev, bufs["recv_high"], slab.next)):
+            ops = [dist.P2POp(dist.isend, send, dst, group), dist.P2POp(dist.irecv, recv, src, group)]
+            for r in dist.batch_isend_irecv(ops):
+                r.wait()
+    backend.rows_set(which, *slab.halo_low(), bufs["recv_low"])
+    backend.rows_set(which, *slab.halo_high(), bufs["recv_high"])
+
+
+def exchange_local(backends, slabs, which, bufs):
+    """The same exchange for all slabs held by one process (one GPU emulating the ranks in turn; no
+    kernel waits for another)."""
+    for b, s, q in zip(backends, slabs, bufs):
+        b.rows_get(which, *s.send_low(), q["send_low"])
+        b.rows_get(which, *s.send_high(), q["send_high"])
+    for b, s, q in zip(backends, slabs, bufs):
+        q["recv_low"].copy_(bufs[s.prev]["send_high"])
+        q["recv_high"].copy_(bufs[s.next]["send_low"])
+    for b, s, q in zip(backends, slabs, bufs):
+        b.rows_set(which, *s.halo_low(), q["recv_low"])
+        b.rows_set(which, *s.halo_high(), q["recv_high"])
+
+
+def rk3_steps(backends, exchange, dt, nsteps, before_step=None):
+    """nsteps decomposed SSP-RK3 steps: before stage s the halo rows of its input buffer (N, A, B) are
+    exchanged, then every slab runs the stage."""
+    for _ in range(nsteps):
+        if before_step is not None:
+            before_step()
+        for s, which in ((1, 0), (2, 1), (3, 2)):
+            exchange(which)
+            for b in backends:
+                b.stage(dt, s)
+    for b in backends:
+        b.sync()
+
+
+class DecomposedModel:
+    """This rank's slab of a workload, advanced with halo exchanges over torch.distributed (one process
+    per GPU, NCCL). interior() is the owned rows' action; gather() assembles the global field on rank 0."""
+
+    def __init__(self, w, precision="fp64", group=None, device=0):
+        import torch
+        import torch.distributed as dist
+        self.group = group
+        world, rank = dist.get_world_size(group), dist.get_rank(group)
+        self.slab = Slab(w.grid.Ny, world, rank)
+        self.local = local_workload(w, self.slab)
+        self.model = self.local.model(precision, device=device)
+        # one stream for the library's kernels, the row copies and the exchange (a stream of its own: the
+        # legacy default stream does not order against the library's non-blocking streams)
+        self.stream = torch.cuda.Stream(device)
+        check(self.model._lib.rpl_set_stream(self.model.handle, _lib.ctypes.c_void_p(self.stream.cuda_stream)))
+        self.backend = LibBackend(self.model)
+        Nk, Np = w.spectral_grid.coordinate_size()
+        self.bufs = _buffers(self.slab, w.grid.Nx, Nk, Np, torch.float32 if precision == "fp32" else torch.float64,
+                             f"cuda:{device}")
+
+    def step(self, dt, nsteps=1):
+        import torch
+        m = self.model
+        check(m._lib.rpl_set_clock(m.handle, m.clock.time, m.clock.iteration))
+        with torch.cuda.stream(self.stream):
+            rk3_steps([self.backend],
+                      lambda which: exchange_dist(self.backend, self.slab, which, self.bufs, self.group),
+                      dt, nsteps, before_step=m._push_field_wind if m._field_wind is not None else None)
+        m.clock.last_Δt = dt
+        return self
+
+    def interior(self):
+        return self.model.action.interior()[:, self.slab.owned()]
+
+    def gather(self):
+        import torch.distributed as dist
+        parts = [None] * self.slab.world
+        dist.all_gather_object(parts, (self.slab.start, self.interior()), group=self.group)
+        return np.concatenate([p for _, p in sorted(parts, key=lambda t: t[0])], axis=1)

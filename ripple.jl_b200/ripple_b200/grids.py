@@ -47,7 +47,7 @@ class RectilinearGrid:
     """
 
     def __init__(self, arch=None, FT=np.float64, *, size, x, y, z=None, halo=(3, 3, 3),
-                 topology=(Periodic, Periodic, Bounded)):
+                 topology=(Periodic, Periodic, Bounded), first_spacings=None):
         size = tuple(int(s) for s in size)
         if len(size) == 2:
             size = size + (0,)
@@ -66,6 +66,9 @@ class RectilinearGrid:
             self._zf = _faces(z, self.Nz, "z")
         else:
             self._zf = np.zeros(0)
+        # (dx, dy) the stencils use, first(xspacings), first(yspacings) unless given (a slab of a larger
+        # uniform grid keeps the parent's values)
+        self._first = None if first_spacings is None else (float(first_spacings[0]), float(first_spacings[1]))
 
     # Oceananigans-style accessors (src/Grids.jl:53-76)
     def xfaces(self):
@@ -85,6 +88,12 @@ class RectilinearGrid:
 
     def znodes(self):
         return 0.5 * (self._zf[:-1] + self._zf[1:]) if self.Nz else np.zeros(0)
+
+    def first_spacings(self):
+        """(first(xspacings), first(yspacings)): the spacings the stencils use."""
+        if self._first is not None:
+            return self._first
+        return float(self.xspacings()[0]), float(self.yspacings()[0])
 
     def xspacings(self):
         return np.diff(self._xf)

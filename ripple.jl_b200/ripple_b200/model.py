@@ -279,8 +279,7 @@ class SpectralWaveModel:
         d.transport = transport
         d.device = int(device)
         d.Nx, d.Ny, d.Nk, d.Np = Nx, Ny, Nk, Np
-        d.dx = float(grid.xspacings()[0])
-        d.dy = float(grid.yspacings()[0])
+        d.dx, d.dy = grid.first_spacings()
         d.xnodes, d.ynodes = dptr(self._keep["x"]), dptr(self._keep["y"])
         d.periodic_x = int(grid.topology[0] == "Periodic")
         d.periodic_y = int(grid.topology[1] == "Periodic")

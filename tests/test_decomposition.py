@@ -1,0 +1,193 @@
+"""Y-slab domain decomposition (ripple_b200.decomposition): slabs with 3 halo rows whose halos are
+refreshed before every RK3 stage reproduce the undecomposed run exactly.
+
+CPU: the oracle advanced slab by slab (its tendency on each halo-extended slab, the RK3 combinations
+of time_step.jl:138-152 stage by stage) with the halo exchange of the library's driver, in one process
+and across 2 and 3 gloo ranks, equals the global oracle run bit for bit. GPU: librpl.so slabs on one
+GPU, exchanged in turn by one process (no kernel waits for another), equal the global model bit for
+bit in FP64 and FP32; a one-rank DecomposedModel too.
+"""
+import os
+import socket
+
+import numpy as np
+import pytest
+
+import ripple_b200 as rp
+from ripple_b200 import decomposition as dc
+from ripple_b200 import workloads
+
+
+def relu(x):
+    return np.where(x > 0.0, x, 0.0)
+
+
+class OracleBackend:
+    """A slab advanced by the oracle: N, A, B like the library's three state buffers."""
+
+    def __init__(self, oracle_mod, w):
+        import torch  # noqa: F401
+        self.o = oracle_mod.Oracle(w)
+        self.N = np.asfortranarray(np.array(w.N0, dtype=np.float64))
+        self.A = np.zeros_like(self.N, order="F")
+        self.B = np.zeros_like(self.N, order="F")
+        self.t = 0.0
+
+    def _arr(self, which):
+        return (self.N, self.A, self.B)[which]
+
+    def rows_get(self, which, first, count, buf):
+        import torch
+        a = self._arr(which)[:, first:first + count]
+        buf.copy_(torch.from_numpy(np.ascontiguousarray(np.transpose(a, (3, 1, 0, 2))).ravel()))
+
+    def rows_set(self, which, first, count, buf):
+        Nx, _, Nk, Np = self.N.shape
+        self._arr(which)[:, first:first + count] = buf.numpy().reshape(Np, count, Nx, Nk).transpose(2, 1, 3, 0)
+
+    def stage(self, dt, s):
+        if s == 1:
+            self.A[...] = relu(self.N + dt * self.o.tendency(self.N, self.t))
+        elif s == 2:
+            st = relu(self.A + dt * self.o.tendency(self.A, self.t))
+            self.B[...] = relu(0.75 * self.N + 0.25 * st)
+        else:
+            st = relu(self.B + dt * self.o.tendency(self.B, self.t))
+            self.N[...] = relu((1.0 / 3.0) * self.N + (2.0 / 3.0) * st)
+            self.t += dt
+
+    def sync(self):
+        pass
+
+
+def cases():
+    return [workloads.seamount_eddies(N=24, Nz=8, Nk=8, Np=12, nsteps=3),   # currents, depth field
+            workloads.hurricane_swell(N=24, Nk=8, Np=12, nsteps=3)]          # sources, moving storm
+
+
+def _buffers(slab, w):
+    import torch
+    Nk, Np = w.spectral_grid.coordinate_size()
+    n = Np * slab.halo * w.grid.Nx * Nk
+    return {k: torch.zeros(n, dtype=torch.float64) for k in ("send_low", "send_high", "recv_low", "recv_high")}
+
+
+# ---------------------------------------------------------------- bookkeeping (CPU)
+
+def test_slabs_cover_the_rows_once():
+    for Ny, world in ((24, 1), (24, 2), (25, 3), (30, 7)):
+        rows = np.concatenate([np.arange(*dc.slab_rows(Ny, world, r)) for r in range(world)])
+        assert np.array_equal(rows, np.arange(Ny))
+        s = dc.Slab(Ny, world, world - 1)
+        g = s.global_rows()
+        assert len(g) == s.rows and g[-1] == 2 and g[s.halo] == s.start
+    with pytest.raises(rp.ArgumentError):
+        dc.Slab(8, 4, 0)                      # 2 rows per rank < 3 halo rows
+
+
+def test_local_grid_keeps_the_parent_geometry():
+    w = cases()[0]
+    s = dc.Slab(24, 3, 1)
+    lw = dc.local_workload(w, s)
+    assert lw.grid.first_spacings() == w.grid.first_spacings()
+    assert np.array_equal(lw.grid.yfaces()[s.halo:s.halo + s.ny + 1], w.grid.yfaces()[s.start:s.stop + 1])
+    assert np.array_equal(lw.N0, w.N0[:, (np.arange(s.start - 3, s.stop + 3) % 24)])
+    assert lw.velocities["u"].shape == (24, s.rows, 8)
+
+
+@pytest.mark.parametrize("case", [0, 1])
+@pytest.mark.parametrize("world", [2, 3])
+def test_oracle_slabs_in_one_process_equal_the_global_run(oracle_mod, case, world):
+    w = cases()[case]
+    slabs = [dc.Slab(w.grid.Ny, world, r) for r in range(world)]
+    backs = [OracleBackend(oracle_mod, dc.local_workload(w, s)) for s in slabs]
+    bufs = [_buffers(s, w) for s in slabs]
+    dc.rk3_steps(backs, lambda which: dc.exchange_local(backs, slabs, which, bufs), w.dt, 3)
+    got = np.concatenate([b.N[:, s.owned()] for b, s in zip(backs, slabs)], axis=1)
+    ref, _ = oracle_mod.Oracle(w).step(w.N0, w.dt, 3)
+    assert np.array_equal(got, ref)
+
+
+def _gloo_rank(rank, world, port, case, out):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"], os.environ["MASTER_PORT"] = "127.0.0.1", str(port)
+    import datetime
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        import oracle as oracle_mod
+        w = cases()[case]
+        slab = dc.Slab(w.grid.Ny, world, rank)
+        back = OracleBackend(oracle_mod, dc.local_workload(w, slab))
+        bufs = _buffers(slab, w)
+        dc.rk3_steps([back], lambda which: dc.exchange_dist(back, slab, which, bufs), w.dt, 3)
+        parts = [None] * world
+        dist.all_gather_object(parts, (slab.start, back.N[:, slab.owned()]))
+        if rank == 0:
+            np.save(out, np.concatenate([p for _, p in sorted(parts, key=lambda t: t[0])], axis=1))
+    finally:
+        dist.destroy_process_group()
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_oracle_slabs_across_gloo_ranks_equal_the_global_run(oracle_mod, tmp_path, world):
+    import torch.multiprocessing as mp
+    out = str(tmp_path / "global.npy")
+    mp.start_processes(_gloo_rank, args=(world, _free_port(), 0, out), nprocs=world, join=True, start_method="spawn")
+    w = cases()[0]
+    ref, _ = oracle_mod.Oracle(w).step(w.N0, w.dt, 3)
+    assert np.array_equal(np.load(out), ref)
+
+
+# ---------------------------------------------------------------- CUDA path (GPU)
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", [0, 1])
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("world", [2, 3])
+def test_library_slabs_on_one_gpu_equal_the_global_model(case, precision, world):
+    import torch
+    w = cases()[case]
+    if precision == "fp32":
+        w.N0 = w.N0.astype(np.float32, order="F")
+    slabs = [dc.Slab(w.grid.Ny, world, r) for r in range(world)]
+    models = [dc.local_workload(w, s).model(precision) for s in slabs]
+    st = torch.cuda.Stream()                       # kernels, row copies and exchange copies in one order
+    for m in models:
+        rp._lib.check(m._lib.rpl_set_stream(m.handle, rp._lib.ctypes.c_void_p(st.cuda_stream)))
+    backs = [dc.LibBackend(m) for m in models]
+    Nk, Np = w.spectral_grid.coordinate_size()
+    dt_t = torch.float32 if precision == "fp32" else torch.float64
+    bufs = [{k: torch.zeros(Np * 3 * w.grid.Nx * Nk, dtype=dt_t, device="cuda")
+             for k in ("send_low", "send_high", "recv_low", "recv_high")} for _ in slabs]
+
+    with torch.cuda.stream(st):
+        dc.rk3_steps(backs, lambda which: dc.exchange_local(backs, slabs, which, bufs), w.dt, 3)
+    got = np.concatenate([m.action.interior()[:, s.owned()] for m, s in zip(models, slabs)], axis=1)
+    g = w.model(precision)
+    rp.time_step(g, w.dt, 3)
+    assert np.array_equal(got, g.action.interior())
+    assert all(m.clock.iteration == 3 for m in models)
+
+
+@pytest.mark.gpu
+def test_one_rank_decomposed_model_equals_the_global_model():
+    import datetime
+    import torch.distributed as dist
+    w = cases()[1]
+    store = dist.TCPStore("127.0.0.1", _free_port(), 1, True)
+    dist.init_process_group("gloo", store=store, rank=0, world_size=1, timeout=datetime.timedelta(seconds=60))
+    try:
+        dm = dc.DecomposedModel(w, "fp64")
+        dm.step(w.dt, 3)
+        got = dm.gather()
+    finally:
+        dist.destroy_process_group()
+    g = w.model("fp64")
+    rp.time_step(g, w.dt, 3)
+    assert np.array_equal(got, g.action.interior())
