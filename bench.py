@@ -67,6 +67,9 @@ def parse():
                          "asynchronous snapshot of the action to pinned host memory every K steps")
     ap.add_argument("--smoothing", action="store_true",
                     help="propagation_smoothing = SpatialAveraging() after every step (the reference's hurricane example)")
+    ap.add_argument("--decompose", action="store_true",
+                    help="one domain split into y slabs over the --gpus ranks with halo exchanges before every RK3 "
+                         "stage (strong scaling); on one GPU it measures the exchange machinery's cost")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
@@ -739,6 +742,62 @@ def run_learned(args, rank, world, local_rank):
     net.close()
 
 
+def run_decomposed(args, rank, world, local_rank):
+    """The workload's one domain split into y slabs, one per rank (ripple_b200.decomposition): halo rows
+    exchanged before every stage (NCCL point-to-point between GPUs; local copies on one rank)."""
+    import datetime
+    import torch
+    import torch.distributed as dist
+    from ripple_b200 import _lib, decomposition
+
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    else:
+        store = dist.TCPStore("127.0.0.1", 0, 1, True)
+        dist.init_process_group("gloo", store=store, rank=0, world_size=1)
+    w = make_workload(args.workload, args.size, args.steps,
+                      n0_dtype=np.float32 if args.precision == "fp32" else np.float64)
+    dm = decomposition.DecomposedModel(w, args.precision, device=local_rank)
+    del w.N0
+    dm.step(w.dt, args.warmup)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    smi_id = "GPU-" + str(torch.cuda.get_device_properties(local_rank).uuid)
+    with ClockSampler(smi_id) as clk:
+        dist.barrier()
+        torch.cuda.synchronize()
+        start.record(dm.stream)
+        dm.step(w.dt, args.steps)
+        end.record(dm.stream)
+        torch.cuda.synchronize()
+        dist.barrier()
+    ms = start.elapsed_time(end)
+    t = torch.tensor([ms], dtype=torch.float64)
+    if world > 1:
+        t = t.cuda()
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    units = w.grid.Nx * w.grid.Ny * dm.model.spectral_grid.coordinate_size()[0] * \
+        dm.model.spectral_grid.coordinate_size()[1]
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": units * args.steps / (ms / 1e3), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32" if args.precision == "fp32" else "f64",
+            "data": DATA.get(args.workload, "synthetic"),
+            "config": {"workload": WORKLOAD_NAMES[args.workload] + " (y-slab decomposition)",
+                       "grid": [args.size, args.size], "spectral": [32, 36], "precision": args.precision,
+                       "units_per_step": units, "parallelism": f"{world} y slabs, 3 halo rows, exchange before "
+                                                              "every stage",
+                       "rows_per_rank": dm.slab.ny},
+            "roofline": None, "cpu_baseline": None, "e2e": None,
+            "gpu_launches": launches_per_step(args.workload) * args.steps, "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    dm.model.close()
+    dist.destroy_process_group()
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -752,6 +811,9 @@ def main():
         return
     if args.workload == "learned":
         run_learned(args, rank, world, local_rank)
+        return
+    if args.decompose:
+        run_decomposed(args, rank, world, local_rank)
         return
     run_ours(args, rank, world, local_rank)
 
