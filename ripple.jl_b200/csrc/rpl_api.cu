@@ -827,7 +827,7 @@ int rpl_diagnostics(rpl_handle* hh, double* m0, double* hs, double* krms, double
     Handle* h = reinterpret_cast<Handle*>(hh);
     cudaStream_t s = h->stream;
     const int64_t P = h->cells;
-    RPL_CUDA(rpl::launch_diagnostics(*h, h->N, s));
+    RPL_CUDA(rpl::launch_diagnostics(*h, h->N, s, hs || krms || mean_dir));
     double* outs[4] = {m0, hs, krms, mean_dir};
     for (int k = 0; k < 4; ++k)
         if (outs[k]) RPL_CUDA(cudaMemcpyAsync(outs[k], h->d_diag + k * P, P * 8, cudaMemcpyDeviceToHost, s));

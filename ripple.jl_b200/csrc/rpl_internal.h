@@ -219,7 +219,8 @@ cudaError_t launch_gradients(const Handle& h, cudaStream_t s);
 cudaError_t launch_cg_field(const Handle& h, cudaStream_t s);
 cudaError_t launch_wind(const Handle& h, double t, cudaStream_t s);
 cudaError_t launch_stress_factor(const Handle& h, const void* Nin, cudaStream_t s, const unsigned int* only = nullptr);
-cudaError_t launch_diagnostics(const Handle& h, const void* Nin, cudaStream_t s);
+// moments = false: m0 and the total action only (Hs, kappa_rms, mean direction left unwritten).
+cudaError_t launch_diagnostics(const Handle& h, const void* Nin, cudaStream_t s, bool moments = true);
 cudaError_t launch_scan_nonfinite(const Handle& h, const void* buf, cudaStream_t s);
 
 // ---- layouts (rpl_layout.cu) ----

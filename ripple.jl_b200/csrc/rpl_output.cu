@@ -149,7 +149,7 @@ int rpl_diagnostics_device(rpl_handle* hh, double* m0, double* hs, double* krms,
     if (st) return st;
     cudaStream_t s = h->stream;
     const int64_t P = h->cells;
-    cudaError_t e = rpl::launch_diagnostics(*h, h->N, s);
+    cudaError_t e = rpl::launch_diagnostics(*h, h->N, s, hs || krms || mean_dir);
     double* outs[4] = {m0, hs, krms, mean_dir};
     for (int k = 0; k < 4 && e == cudaSuccess; ++k)
         if (outs[k]) e = cudaMemcpyAsync(outs[k], h->d_diag + k * P, P * 8, cudaMemcpyDeviceToDevice, s);

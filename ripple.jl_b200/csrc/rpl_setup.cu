@@ -265,7 +265,8 @@ __device__ __forceinline__ void tadd(double& s, double& c, double v) {
 // (coalesced reads of each direction's kappa column); per lane, FP64 sums of blocks of 4 directions
 // folded into compensated totals, then a fixed-order compensated butterfly over the lanes
 // (deterministic). The error stays within a few units in the last place of the sum of |terms|.
-template <typename T>
+// ALL = false computes m0 alone (for the total action), with the same arithmetic for m0.
+template <typename T, bool ALL>
 __global__ void __launch_bounds__(256)
 diag_kernel(const T* __restrict__ N, int64_t Nx, int64_t Ny, int64_t Nk, int64_t Np,
             const double* __restrict__ tabs, double* __restrict__ out) {
@@ -299,14 +300,18 @@ diag_kernel(const T* __restrict__ N, int64_t Nx, int64_t Ny, int64_t Nk, int64_t
 #pragma unroll
             for (int k = 0; k < DB; ++k) {
                 b0 = fma(a[k], __ldg(w + b[k]), b0);
-                bx = fma(a[k], __ldg(mux + b[k]), bx);
-                by = fma(a[k], __ldg(muy + b[k]), by);
-                bt = fma(a[k], __ldg(tr + b[k]), bt);
+                if (ALL) {
+                    bx = fma(a[k], __ldg(mux + b[k]), bx);
+                    by = fma(a[k], __ldg(muy + b[k]), by);
+                    bt = fma(a[k], __ldg(tr + b[k]), bt);
+                }
             }
             tadd(s0, c0, b0);
-            tadd(sx, cx, bx);
-            tadd(sy, cy, by);
-            tadd(st, ct, bt);
+            if (ALL) {
+                tadd(sx, cx, bx);
+                tadd(sy, cy, by);
+                tadd(st, ct, bt);
+            }
         }
     }
 #pragma unroll
@@ -314,22 +319,27 @@ diag_kernel(const T* __restrict__ N, int64_t Nx, int64_t Ny, int64_t Nk, int64_t
         double so = __shfl_down_sync(0xffffffffu, s0, off), co = __shfl_down_sync(0xffffffffu, c0, off);
         tadd(s0, c0, so);
         c0 += co;
-        so = __shfl_down_sync(0xffffffffu, sx, off), co = __shfl_down_sync(0xffffffffu, cx, off);
-        tadd(sx, cx, so);
-        cx += co;
-        so = __shfl_down_sync(0xffffffffu, sy, off), co = __shfl_down_sync(0xffffffffu, cy, off);
-        tadd(sy, cy, so);
-        cy += co;
-        so = __shfl_down_sync(0xffffffffu, st, off), co = __shfl_down_sync(0xffffffffu, ct, off);
-        tadd(st, ct, so);
-        ct += co;
+        if (ALL) {
+            so = __shfl_down_sync(0xffffffffu, sx, off), co = __shfl_down_sync(0xffffffffu, cx, off);
+            tadd(sx, cx, so);
+            cx += co;
+            so = __shfl_down_sync(0xffffffffu, sy, off), co = __shfl_down_sync(0xffffffffu, cy, off);
+            tadd(sy, cy, so);
+            cy += co;
+            so = __shfl_down_sync(0xffffffffu, st, off), co = __shfl_down_sync(0xffffffffu, ct, off);
+            tadd(st, ct, so);
+            ct += co;
+        }
     }
     if (lane == 0) {
-        const double m0 = s0 + c0, mx = sx + cx, my = sy + cy, mt = st + ct;
+        const double m0 = s0 + c0;
         out[c] = m0;
-        out[P + c] = 4.0 * sqrt(m0);
-        out[2 * P + c] = sqrt(m0 == 0.0 ? 0.0 : mt / m0);
-        out[3 * P + c] = atan2(my, mx);
+        if (ALL) {
+            const double mx = sx + cx, my = sy + cy, mt = st + ct;
+            out[P + c] = 4.0 * sqrt(m0);
+            out[2 * P + c] = sqrt(m0 == 0.0 ? 0.0 : mt / m0);
+            out[3 * P + c] = atan2(my, mx);
+        }
     }
 }
 
@@ -522,15 +532,25 @@ cudaError_t launch_stress_factor(const Handle& h, const void* Nin, cudaStream_t 
     return cudaGetLastError();
 }
 
-cudaError_t launch_diagnostics(const Handle& h, const void* Nin, cudaStream_t s) {
+cudaError_t launch_diagnostics(const Handle& h, const void* Nin, cudaStream_t s, bool moments) {
     const rpl_desc& d = h.desc;
     const int64_t P = d.Nx * d.Ny;
-    if (h.precision == RPL_FP64)
-        diag_kernel<double><<<blocks_for(P * 32, 256), 256, 0, s>>>((const double*)Nin, d.Nx, d.Ny, d.Nk, d.Np,
-                                                                    h.d_weights, h.d_diag);
-    else
-        diag_kernel<float><<<blocks_for(P * 32, 256), 256, 0, s>>>((const float*)Nin, d.Nx, d.Ny, d.Nk, d.Np,
-                                                                   h.d_weights, h.d_diag);
+    const unsigned blocks = blocks_for(P * 32, 256);
+    if (h.precision == RPL_FP64) {
+        if (moments)
+            diag_kernel<double, true><<<blocks, 256, 0, s>>>((const double*)Nin, d.Nx, d.Ny, d.Nk, d.Np, h.d_weights,
+                                                             h.d_diag);
+        else
+            diag_kernel<double, false><<<blocks, 256, 0, s>>>((const double*)Nin, d.Nx, d.Ny, d.Nk, d.Np,
+                                                              h.d_weights, h.d_diag);
+    } else {
+        if (moments)
+            diag_kernel<float, true><<<blocks, 256, 0, s>>>((const float*)Nin, d.Nx, d.Ny, d.Nk, d.Np, h.d_weights,
+                                                            h.d_diag);
+        else
+            diag_kernel<float, false><<<blocks, 256, 0, s>>>((const float*)Nin, d.Nx, d.Ny, d.Nk, d.Np, h.d_weights,
+                                                             h.d_diag);
+    }
     total_kernel<<<1, 1024, 0, s>>>(h.d_diag, P, d.dx * d.dy, h.d_diag + 4 * P);
     return cudaGetLastError();
 }

@@ -79,3 +79,16 @@ def test_diagnostics_device_equal_host_diagnostics():
     for k, f in zip(("m0", "Hs", "kappa_rms", "mean_direction"), fields):
         assert np.array_equal(f.cpu().numpy().reshape((Nx, Ny), order="F"), d[k]), k
     assert series[1].item() == d["total_action"] and series[0].item() == 0.0
+
+
+def test_total_only_diagnostics_equal_the_full_call():
+    """A call that asks for m0 and the total action alone takes the m0-only kernel: same values, bit for
+    bit, as the full call."""
+    w, m = small("fp32")
+    rp.time_step(m, w.dt, 2)
+    full = rp.diagnostics(m.action)
+    m0 = np.empty((m.grid.Nx, m.grid.Ny), order="F")
+    tot = np.zeros(1)
+    rp._lib.check(m._lib.rpl_diagnostics(m.handle, rp._lib.dptr(m0), None, None, None, rp._lib.dptr(tot)))
+    assert np.array_equal(m0, full["m0"])
+    assert tot[0] == full["total_action"]
