@@ -134,12 +134,13 @@ def _free_port():
         return s.getsockname()[1]
 
 
-@pytest.mark.parametrize("world", [2, 3])
-def test_oracle_slabs_across_gloo_ranks_equal_the_global_run(oracle_mod, tmp_path, world):
+@pytest.mark.parametrize("world,case", [(2, 0), (3, 0), (2, 1)])
+def test_oracle_slabs_across_gloo_ranks_equal_the_global_run(oracle_mod, tmp_path, world, case):
     import torch.multiprocessing as mp
     out = str(tmp_path / "global.npy")
-    mp.start_processes(_gloo_rank, args=(world, _free_port(), 0, out), nprocs=world, join=True, start_method="spawn")
-    w = cases()[0]
+    mp.start_processes(_gloo_rank, args=(world, _free_port(), case, out), nprocs=world, join=True,
+                       start_method="spawn")
+    w = cases()[case]
     ref, _ = oracle_mod.Oracle(w).step(w.N0, w.dt, 3)
     assert np.array_equal(np.load(out), ref)
 
