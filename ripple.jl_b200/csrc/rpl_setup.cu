@@ -287,13 +287,13 @@ diag_kernel(const T* __restrict__ N, int64_t Nx, int64_t Ny, int64_t Nk, int64_t
         // blocks of DB directions: the block's loads are issued together, its terms summed with FMAs,
         // and the block sum folded into the compensated totals
         constexpr int DB = 4;
-        for (int n0 = 0; n0 < np; n0 += DB, p += DB * stride) {
+        auto block = [&](int n0, const T* q) {
             double a[DB];
             int b[DB];
 #pragma unroll
             for (int k = 0; k < DB; ++k) {
                 const bool in = n0 + k < np;
-                a[k] = in ? (double)p[k * stride] : 0.0;
+                a[k] = in ? (double)q[k * stride] : 0.0;
                 b[k] = in ? m + nk * (n0 + k) : m;  // a[k] = 0 past the last direction
             }
             double b0 = 0.0, bx = 0.0, by = 0.0, bt = 0.0;
@@ -312,6 +312,13 @@ diag_kernel(const T* __restrict__ N, int64_t Nx, int64_t Ny, int64_t Nk, int64_t
                 tadd(sy, cy, by);
                 tadd(st, ct, bt);
             }
+        };
+        if (ALL) {
+            for (int n0 = 0; n0 < np; n0 += DB, p += DB * stride) block(n0, p);
+        } else {
+            // m0 alone has registers to spare: two blocks' loads in flight, the same summation order
+#pragma unroll 2
+            for (int n0 = 0; n0 < np; n0 += DB, p += DB * stride) block(n0, p);
         }
     }
 #pragma unroll
