@@ -56,6 +56,9 @@ def parse():
                     help="share of cells without source activity kept as training rows (--workload learned)")
     ap.add_argument("--members", type=int, default=64, help="ensemble members (--workload ensemble)")
     ap.add_argument("--autotune-cache", default="", help="tile-shape cache file (--workload ensemble)")
+    ap.add_argument("--direct-cells", type=int, default=65536,
+                    help="ensemble members of at least this many cells take their own single-model stage launches "
+                         "inside the captured step; 0: all members in the persistent launches (--workload ensemble)")
     ap.add_argument("--member-sizes", default="64,128,256,384",
                     help="grid sizes the ensemble members are drawn from (--workload ensemble)")
     ap.add_argument("--size", type=int, default=0, help="grid points per side (default 1024 / 768)")
@@ -478,7 +481,7 @@ def run_ensemble(args, rank, world, local_rank):
     t_build = time.perf_counter() - t_build
     cache = args.autotune_cache or None
     t_tune = time.perf_counter()
-    ens = rp.Ensemble(models, dts, use_graph=True, autotune=True, autotune_cache=cache)
+    ens = rp.Ensemble(models, dts, use_graph=True, autotune=True, autotune_cache=cache, direct_cells=args.direct_cells)
     t_tune = time.perf_counter() - t_tune
     lib, h = ens._lib, ens.handle
     units = ens.units
@@ -559,20 +562,12 @@ def run_ensemble(args, rank, world, local_rank):
             "data": "synthetic (seeded members: seamount depth, vortex or eddy currents U0 0.1-0.8 m/s, JONSWAP N0)",
             "config": {"workload": "ensemble_members", "members": len(models), "seed": 4, "member_sizes": sizes,
                        "units_per_step": units, "classes": {k: {"count": v[0], "tile": v[1]} for k, v in classes.items()},
+                       "direct_cells": args.direct_cells,
                        "sequential_ms_per_step": ms_seq / args.steps,
                        "speedup_vs_sequential": ms_seq / ms,
                        "build_s": t_build, "autotune_s": t_tune,
                        "l2": "state (%.1f GB per buffer set) larger than L2; no flush" % (4 * units / 1e9),
-                       "parallelism": f"{world} independent replicas" if world > 1 else "1 GPU",
-                       **({"currents": "time-varying: new u, v every step (Q transform + gradients + coefficients "
-                                       "in the timed region)", "currents_refresh_ms": refresh_ms} if cur else {}),
-                       **({"propagation_smoothing": "SpatialAveraging(αs=0.5, αn=0.5) after every step"}
-                          if args.smoothing else {}),
-                       **({"output": {"diagnostics": "total action into a device time series every step",
-                                      "snapshot_every": args.output_every,
-                                      "snapshot_bytes": snap_bufs[0].array.nbytes,
-                                      "snapshot_copy_after_timed_region_ms": snap_tail_ms}}
-                          if snap_bufs is not None else {})},
+                       "parallelism": f"{world} independent replicas" if world > 1 else "1 GPU"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": None, "peak_kind": peak_kind, "kernel": "ensemble_kernel",
                          "launch_ms": launch_ms, "algorithmic_bytes_per_launch": nbytes_alg / 3.0,

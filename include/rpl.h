@@ -268,7 +268,9 @@ typedef struct rpl_ensemble_options {
     int32_t abi_version;          /* RPL_ABI_VERSION */
     int32_t use_graph;            /* 1: replay one captured CUDA graph per step; 0: three launches */
     int32_t autotune;             /* 1: tune size classes missing from the cache during creation */
-    int32_t reserved;
+    int32_t direct_cells;         /* > 0: members of at least this many cells (Nx*Ny) take their own
+                                     single-model stage launches inside the step, the rest share the
+                                     persistent launches; 0: every member in the persistent launches */
     const char* autotune_cache;   /* text file of tuned shapes, read at creation and appended to by
                                      the autotuner; NULL: no file */
 } rpl_ensemble_options;

@@ -35,6 +35,8 @@ struct rpl_ensemble {
     std::vector<Handle*> members;
     std::vector<double> dt;
     std::vector<int> shape;             // per member: index into kEnsembleShapes
+    int64_t direct_cells = 0;           // members with at least this many cells take single-model launches
+    std::vector<char> direct;           // per member: stages launched directly, not in the persistent kernel
     std::vector<std::string> key;       // per member: size-class key
     TileArgs* d_args = nullptr;         // [3][count]: stage-major
     int4* d_items = nullptr;
@@ -140,26 +142,41 @@ int upload_items(rpl_ensemble* e, const std::vector<int>& which, int force_shape
         ENS_CUDA(cudaMalloc((void**)&e->d_items, items.size() * sizeof(int4)));
         e->item_capacity = items.size();
     }
-    ENS_CUDA(cudaMemcpyAsync(e->d_items, items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice,
-                             e->stream));
-    ENS_CUDA(cudaStreamSynchronize(e->stream));
+    if (!items.empty()) {
+        ENS_CUDA(cudaMemcpyAsync(e->d_items, items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice,
+                                 e->stream));
+        ENS_CUDA(cudaStreamSynchronize(e->stream));
+    }
     e->nitems = (int)items.size();
     return RPL_OK;
 }
 
+// The persistent launches' items: every member that does not take direct launches.
 int all_items(rpl_ensemble* e) {
-    std::vector<int> all(e->members.size());
-    for (size_t m = 0; m < all.size(); ++m) all[m] = (int)m;
+    std::vector<int> all;
+    for (size_t m = 0; m < e->members.size(); ++m)
+        if (!e->direct[m]) all.push_back((int)m);
     drop_graph(e);
     return upload_items(e, all, -1);
 }
 
+// One RK3 step: per stage, the direct members' single-model stage launches (each fills the GPU on its
+// own), then one persistent launch over the other members' tiles.
 cudaError_t enqueue_step(rpl_ensemble* e) {
     const size_t M = e->members.size();
     cudaError_t err = cudaMemsetAsync(e->d_counters, 0, 3 * sizeof(unsigned int), e->stream);
-    for (int s = 0; s < 3 && err == cudaSuccess; ++s)
-        err = rpl::launch_ensemble_stage(e->refract, e->d_args + s * M, e->d_items, e->nitems, e->d_counters + s,
-                                         e->grid, e->stream);
+    for (int s = 0; s < 3 && err == cudaSuccess; ++s) {
+        for (size_t m = 0; m < M && err == cudaSuccess; ++m) {
+            if (!e->direct[m]) continue;
+            const Handle& h = *e->members[m];
+            const void* Nin = s == 0 ? h.N : (s == 1 ? h.A : h.B);
+            void* Nout = s == 0 ? h.A : (s == 1 ? h.B : h.N);
+            err = rpl::launch_stage(h, rpl::make_params(h, e->dt[m], s + 1), Nin, h.N, Nout, e->stream);
+        }
+        if (err == cudaSuccess && e->nitems > 0)
+            err = rpl::launch_ensemble_stage(e->refract, e->d_args + s * M, e->d_items, e->nitems,
+                                             e->d_counters + s, e->grid, e->stream);
+    }
     return err;
 }
 
@@ -355,6 +372,13 @@ int rpl_ensemble_create(rpl_handle* const* members, const double* dt, int32_t co
     e->cache = (options && options->autotune_cache) ? options->autotune_cache : "";
     e->members = hs;
     e->dt.assign(dt, dt + count);
+    e->direct_cells = options ? options->direct_cells : 0;
+    if (e->direct_cells < 0) {
+        destroy(e);
+        return efail(RPL_ERR_ARGUMENT, "direct_cells must be >= 0");
+    }
+    for (int i = 0; i < count; ++i)
+        e->direct.push_back(e->direct_cells > 0 && hs[i]->cells >= e->direct_cells ? 1 : 0);
     const std::map<std::string, int> cached = read_cache(e->cache);
     for (int i = 0; i < count; ++i) {
         e->key.push_back(class_key(*hs[i], e->device));

@@ -56,7 +56,7 @@ class RplSources(ctypes.Structure):
 
 
 class RplEnsembleOptions(ctypes.Structure):
-    _fields_ = [("abi_version", _i32), ("use_graph", _i32), ("autotune", _i32), ("reserved", _i32),
+    _fields_ = [("abi_version", _i32), ("use_graph", _i32), ("autotune", _i32), ("direct_cells", _i32),
                 ("autotune_cache", ctypes.c_char_p)]
 
 

@@ -21,7 +21,7 @@ class Ensemble:
     candidate tile shapes of every size class at creation (cached in `autotune_cache` if given).
     """
 
-    def __init__(self, models, dts, use_graph=True, autotune=False, autotune_cache=None):
+    def __init__(self, models, dts, use_graph=True, autotune=False, autotune_cache=None, direct_cells=0):
         models = list(models)
         dts = np.ascontiguousarray(np.broadcast_to(np.asarray(dts, dtype=np.float64), (len(models),)))
         if not models:
@@ -31,8 +31,8 @@ class Ensemble:
         self.dts = dts
         handles = (ctypes.c_void_p * len(models))(*[m.handle.value for m in models])
         self._cache = autotune_cache.encode() if autotune_cache else None
-        opts = _lib.RplEnsembleOptions(_lib.RPL_ABI_VERSION, 1 if use_graph else 0, 1 if autotune else 0, 0,
-                                       self._cache)
+        opts = _lib.RplEnsembleOptions(_lib.RPL_ABI_VERSION, 1 if use_graph else 0, 1 if autotune else 0,
+                                       int(direct_cells), self._cache)
         h = ctypes.c_void_p()
         for m in models:
             check(self._lib.rpl_set_clock(m.handle, m.clock.time, m.clock.iteration))

@@ -53,6 +53,28 @@ def test_ensemble_matches_members_run_alone_and_oracle(oracle_mod):
     ens.close()
 
 
+@pytest.mark.parametrize("direct_cells", [1000, 1])
+def test_direct_members_equal_their_own_runs(direct_cells):
+    """Members of at least direct_cells cells take their own single-model stage launches inside the
+    captured step (bit-identical to running alone); the others share the persistent launches (1: all
+    members direct, no persistent launch)."""
+    ws = member_workloads(nsteps=2)
+    models = [w.model("fp32") for w in ws]
+    ens = rp.Ensemble(models, [w.dt for w in ws], direct_cells=direct_cells)
+    ens.time_step(2)
+    for w, m in zip(ws, models):
+        a = w.model("fp32")
+        rp.time_step(a, w.dt, 2)
+        ref = a.action.interior()
+        if w.grid.Nx * w.grid.Ny >= direct_cells:
+            assert np.array_equal(m.action.interior(), ref)
+        else:
+            assert np.max(np.abs(m.action.interior() - ref)) <= 1e-6 * np.max(np.abs(ref))
+        assert m.clock.iteration == 2
+        a.close()
+    ens.close()
+
+
 def test_ensemble_graph_plain_and_sequential_agree():
     ws = member_workloads(nsteps=2)
     results = []
