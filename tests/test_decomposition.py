@@ -95,6 +95,23 @@ def test_local_grid_keeps_the_parent_geometry():
     assert lw.velocities["u"].shape == (24, s.rows, 8)
 
 
+def test_local_workload_rejects_what_is_not_decomposed():
+    s = dc.Slab(24, 2, 0)
+    w = cases()[0]
+    w.propagation_smoothing = rp.SpatialAveraging()
+    with pytest.raises(rp.ArgumentError):
+        dc.local_workload(w, s)                       # the averaging needs an exchange after stage 3
+    w = workloads.self_coupled_swell(N=24, Nk=8, Np=12)
+    with pytest.raises(rp.ArgumentError):
+        dc.local_workload(w, s)                       # pseudomomentum coupling
+    w = cases()[1]
+    g = w.grid
+    w.grid = rp.RectilinearGrid(size=(g.Nx, g.Ny, g.Nz), x=g.xfaces(), y=g.yfaces(), z=g.zfaces(),
+                                topology=("Periodic", "Bounded", "Bounded"))
+    with pytest.raises(rp.ArgumentError):
+        dc.local_workload(w, s)                       # a bounded y axis
+
+
 @pytest.mark.parametrize("case", [0, 1])
 @pytest.mark.parametrize("world", [2, 3])
 def test_oracle_slabs_in_one_process_equal_the_global_run(oracle_mod, case, world):
