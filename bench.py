@@ -73,6 +73,9 @@ def parse():
     ap.add_argument("--decompose", action="store_true",
                     help="one domain split into y slabs over the --gpus ranks with halo exchanges before every RK3 "
                          "stage (strong scaling); on one GPU it measures the exchange machinery's cost")
+    ap.add_argument("--accuracy-steps", type=int, default=-1,
+                    help="FP32 precision form: steps of the accuracy arm (FP32 and FP64 runs from the same start, "
+                         "compared on the device); -1: the configuration's own step count, 0: off")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
@@ -81,6 +84,7 @@ def parse():
     return args
 
 
+CONFIG_STEPS = {"seamount": 200, "hurricane": 1000, "selfcoupled": 200}   # RK3 steps of each configuration
 WORKLOAD_NAMES = {"seamount": "seamount_eddies", "hurricane": "hurricane_swell", "ensemble": "ensemble_members",
                   "learned": "hurricane_swell (learned source)", "selfcoupled": "self_coupled_swell"}
 TRAFFIC_SUFFIX = {"seamount": "", "hurricane": "_hurricane", "selfcoupled": "_selfcoupled"}
@@ -191,49 +195,117 @@ def algorithmic_bytes(w, precision):
     return 8 * s * w.units + tables + extra
 
 
-def cpu_baseline(name, steps=4, n=128):
-    """The oracle (FP64 C++ restatement of the reference CPU path, OpenMP) on a bounded sample."""
+CPU_GRID = 96          # CPU sample grid: the workload's physics and spectral grid on 96^2 cells
+
+
+def cpu_sample(name, steps, warmup=1, threads=None, n=CPU_GRID):
+    """The reference CPU path (the oracle: FP64 C++ restatement, OpenMP over columns) on a bounded
+    sample of the workload: `warmup` untimed then `steps` timed RK3 steps on an n^2 grid with the same
+    physics and spectral grid. threads=None: every host thread OpenMP offers. Returns (units/s, s,
+    threads used, sample description)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
-    w = make_workload(name, n, steps)
-    o = oracle.Oracle(w)
-    o.step(w.N0, w.dt, 1)
-    t = time.perf_counter()
-    o.step(w.N0, w.dt, steps)
-    el = time.perf_counter() - t
-    return {"value": w.units * steps / el, "unit": UNIT, "cores": oracle.num_threads(), "kind": "port",
-            "sample": f"{WORKLOAD_NAMES[name]} at {n}^2 x 32 kappa x 36 phi (same physics, reduced grid), "
-                      f"{steps} RK3 steps FP64, {el:.1f} s"}
+    full = oracle.num_threads()
+    oracle.set_threads(threads or full)
+    try:
+        w = make_workload(name, n, steps)
+        o = oracle.Oracle(w)
+        N = w.N0
+        for _ in range(warmup):
+            N, _ = o.step(N, w.dt, 1)
+        t = time.perf_counter()
+        for _ in range(steps):
+            N, _ = o.step(N, w.dt, 1)
+        el = time.perf_counter() - t
+        used = oracle.num_threads()
+    finally:
+        oracle.set_threads(full)
+    sample = (f"{WORKLOAD_NAMES[name]} at {n}^2 x 32 kappa x 36 phi (same physics, reduced grid), "
+              f"{steps} FP64 RK3 steps after {warmup} warm-up, {used} thread(s), {el:.1f} s")
+    return w.units * steps / el, el, used, sample
+
+
+def cpu_baseline(name, steps):
+    """cpu_baseline of the GPU line: the same sample as the --impl reference arm (same grid, same step
+    count) on all host threads, plus a shorter 1-thread sample."""
+    v, el, used, sample = cpu_sample(name, steps)
+    v1, el1, _, sample1 = cpu_sample(name, max(1, min(2, steps)), threads=1)
+    return {"value": v, "unit": UNIT, "cores": used, "kind": "port", "sample": sample,
+            "one_thread": {"value": v1, "unit": UNIT, "cores": 1, "sample": sample1}}
 
 
 def run_reference(args, rank):
     if rank != 0:
         return
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle
-    n = 96
-    w = make_workload(args.workload, n, 1)
-    o = oracle.Oracle(w)
-    N = w.N0
-    for _ in range(args.warmup):
-        N, _ = o.step(N, w.dt, 1)
-    t = time.perf_counter()
-    for _ in range(args.steps):
-        N, _ = o.step(N, w.dt, 1)
-    el = time.perf_counter() - t
-    value = w.units * args.steps / el
-    sample = (f"each step one FP64 SSP-RK3 step of {WORKLOAD_NAMES[args.workload]} at {n}^2 x 32 kappa x 36 phi "
-              f"({args.size}^2 does not fit a bounded CPU sample); per-unit throughput")
+    value, el, used, sample = cpu_sample(args.workload, args.steps, warmup=args.warmup)
+    sample += f" ({args.size}^2 does not fit a bounded CPU sample); per-unit throughput"
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
             "impl": "reference",
-            "config": {"workload": WORKLOAD_NAMES[args.workload], "grid": [n, n], "spectral": [32, 36],
+            "config": {"workload": WORKLOAD_NAMES[args.workload], "grid": [CPU_GRID, CPU_GRID], "spectral": [32, 36],
                        "precision": "fp64", "path": "reference CPU path restated in C++ (oracle/), OpenMP"},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": oracle.num_threads(), "kind": "port",
-                             "sample": sample},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": used, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def device_state(m, precision, torch, _lib):
+    """The model's action as a CUDA tensor, caller layout (x fastest)."""
+    t = torch.empty(m.action.size if isinstance(m.action.size, int) else int(np.prod(m.action.size)),
+                    dtype=torch.float32 if precision == "fp32" else torch.float64, device=f"cuda:{m.device}")
+    _lib.check(m._lib.rpl_get_action_device(m.handle, _lib.ctypes.c_void_p(t.data_ptr()),
+                                            _lib.RPL_F32 if precision == "fp32" else _lib.RPL_F64, 0))
+    return t
+
+
+def rel_l2_device(a, b, torch, chunk=1 << 27):
+    num = den = 0.0
+    for s in range(0, a.numel(), chunk):
+        x, y = a[s:s + chunk].double(), b[s:s + chunk].double()
+        num += float(torch.sum((x - y) ** 2))
+        den += float(torch.sum(y * y))
+    return math.sqrt(num / den)
+
+
+def accuracy_arm(w, steps, local_rank):
+    """The precision form against the plain FP64 GPU path (pinned to the CPU oracle on reduced grids):
+    FP32 and FP64 models run `steps` RK3 steps from the same initial action; the last steps - 3 of each
+    are device-timed (CUDA events on the model's stream); final actions, Hs and total actions are
+    compared on the device. Drift = change of the total action over the run / its initial value."""
+    import torch
+    import ripple_b200 as rp
+    from ripple_b200 import _lib
+    warm = min(3, max(0, steps - 1))
+    res = {}
+    for prec in ("fp32", "fp64"):
+        m = w.model(prec, device=local_rank)
+        stream = torch.cuda.Stream(device=local_rank)
+        _lib.check(m._lib.rpl_set_stream(m.handle, _lib.ctypes.c_void_p(stream.cuda_stream)))
+        t0 = rp.total_action(m.action)
+        _lib.check(m._lib.rpl_step_async(m.handle, w.dt, warm))
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        _lib.check(m._lib.rpl_step_async(m.handle, w.dt, steps - warm))
+        b.record(stream)
+        stream.synchronize()
+        _lib.check(m._lib.rpl_sync(m.handle))
+        m._sync_clock()
+        d = rp.diagnostics(m.action)
+        res[prec] = dict(ms=a.elapsed_time(b) / (steps - warm), N=device_state(m, prec, torch, _lib), Hs=d["Hs"],
+                         t0=t0, t1=d["total_action"])
+        m.close()
+    f, g = res["fp32"], res["fp64"]
+    out = {"steps": steps, "timed_steps": steps - warm,
+           "rel_l2_vs_fp64": rel_l2_device(f["N"], g["N"], torch),
+           "hs_rel_l2_vs_fp64": float(np.linalg.norm(f["Hs"] - g["Hs"]) / np.linalg.norm(g["Hs"])),
+           "total_action_rel_diff_vs_fp64": abs(f["t1"] - g["t1"]) / abs(g["t1"]),
+           "action_drift": (f["t1"] - f["t0"]) / f["t0"], "action_drift_fp64": (g["t1"] - g["t0"]) / g["t0"],
+           "fp32_ms_per_step": f["ms"], "fp64_ms_per_step": g["ms"],
+           "reference": "plain FP64 GPU path, pinned to the CPU FP64 oracle at <= 1e-12 (128^2, 20 steps)"}
+    del res
+    torch.cuda.empty_cache()
+    return out
 
 
 def run_ours(args, rank, world, local_rank):
@@ -401,9 +473,15 @@ def run_ours(args, rank, world, local_rank):
                "includes": "set! from pinned host, K x (" + ("new currents from pinned host + " if cur else "") +
                            "time_step! + total_action read), interior to pinned host"}
 
+    m.close()
+    acc = None
+    acc_steps = CONFIG_STEPS.get(args.workload, 0) if args.accuracy_steps < 0 else args.accuracy_steps
+    if args.precision == "fp32" and acc_steps > 0 and not (cur or snap_bufs or args.smoothing):
+        acc = accuracy_arm(w, acc_steps, local_rank)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_baseline(args.workload)
+        cpu = cpu_baseline(args.workload, args.steps)
 
     if rank == 0:
         line = {
@@ -433,13 +511,15 @@ def run_ours(args, rank, world, local_rank):
                                                                "selfcoupled": " incl. its coupling refresh"}.get(
                                                                    args.workload, " incl. its wind/stress-cap kernels")},
             "cpu_baseline": cpu, "e2e": e2e,
+            **({"rel_l2_vs_fp64": acc["rel_l2_vs_fp64"], "action_drift": acc["action_drift"],
+                "fp64_ms_per_step": acc["fp64_ms_per_step"],
+                "speedup_vs_fp64": acc["fp64_ms_per_step"] / (ms / args.steps), "accuracy": acc} if acc else {}),
             "gpu_launches": (launches_per_step(args.workload) + (3 if cur else 0) + (2 if snap_bufs else 0)
                              + (1 if args.smoothing else 0)) * args.steps
                             + (args.steps // args.output_every if snap_bufs else 0),
             "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
-    m.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
@@ -550,7 +630,7 @@ def run_ensemble(args, rank, world, local_rank):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_baseline("ensemble", steps=20, n=64)
+        cpu = cpu_baseline("ensemble", args.steps)
     if rank == 0:
         classes = {}
         for (N, (Nk, Np)), shp in zip(shapes_info, ens.shapes()):

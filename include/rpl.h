@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define RPL_ABI_VERSION 1
+#define RPL_ABI_VERSION 2
 
 typedef struct rpl_handle rpl_handle;
 
@@ -88,6 +88,8 @@ typedef struct rpl_desc {
     const double* depth_field;  /* Nx*Ny */
     double gravity;             /* 9.81 in the reference */
     int64_t memory_limit_bytes; /* 0: no limit; else creation fails with RPL_ERR_OOM above it */
+    const double* xspacings;    /* Nx cell widths Δx(i) and Ny cell heights Δy(j): the total action sums */
+    const double* yspacings;    /* m0(i,j)·Δx(i)·Δy(j) (diagnostic_operations.jl:492-503); NULL: dx, dy */
 } rpl_desc;
 
 /* Source bundle: PrecomputedSources(wind_input=PressureCorrelationInput(...),
@@ -243,7 +245,9 @@ int rpl_host_free(void* ptr);
  * and total (1 value) may each be NULL. Kernels go on `stream` (a cudaStream_t, NULL = default).
  * The only scratch, the per-block partial sums of the total action, is a fixed 256 KiB array inside
  * the library that every GPU loading librpl.so keeps until the process exits, so Nx*Ny is limited to
- * RPL_STATIC_MAX_COLUMNS (larger grids return RPL_ERR_ARGUMENT). Every call reuses that array, so
+ * RPL_STATIC_MAX_COLUMNS (larger grids return RPL_ERR_ARGUMENT). dx and dy are the cell widths of a
+ * uniform horizontal grid (every cell's area is dx*dy in the total); a stretched grid's total action
+ * needs rpl_diagnostics, which takes each cell's own widths. Every call reuses that array, so
  * calls that may overlap on the GPU (different streams, different host threads) race and must be
  * ordered by the caller. The first call on each device looks up the array's device address and may
  * load the library's kernels onto that device; make that first call before any stream capture. */

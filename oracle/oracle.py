@@ -40,7 +40,8 @@ class OraModel(ctypes.Structure):
                 ("von_karman", _d), ("gravity", _d), ("has_dissipation", _i32), ("C_ds", _d), ("B_r", _d),
                 ("ds_p", _d), ("sigma_power", _d), ("ds_gravity", _d), ("pm_mode", _i32), ("pm_per_cell", _i32),
                 ("pm_overlap", _dp), ("pm_kx", _dp), ("pm_ky", _dp), ("gse", _i32), ("periodic_x", _i32),
-                ("periodic_y", _i32), ("gse_alpha_s", _d), ("gse_alpha_n", _d)]
+                ("periodic_y", _i32), ("gse_alpha_s", _d), ("gse_alpha_n", _d), ("xspacings", _dp),
+                ("yspacings", _dp)]
 
 
 def build():
@@ -163,6 +164,8 @@ class Oracle:
         m.dx, m.dy = g.first_spacings() if hasattr(g, "first_spacings") else (float(g.xspacings()[0]),
                                                                               float(g.yspacings()[0]))
         m.xnodes, m.ynodes = p(self._x), p(self._y)
+        self._xsp, self._ysp = f64(g.xspacings()), f64(g.yspacings())
+        m.xspacings, m.yspacings = p(self._xsp), p(self._ysp)
         m.kappa, m.kappa_faces, m.phi, m.phi_faces, m.weights = p(k), p(self._kf), p(ph), p(self._pf), p(self._w)
         depth = w.depth
         infinite = type(depth).__name__ == "InfiniteDepth"

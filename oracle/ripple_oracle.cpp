@@ -786,7 +786,8 @@ void ora_rk3_step(const ora_model* M, double* N, double dt, int64_t nsteps, doub
 /* src/Diagnostics/moments.jl:33-37,100-123; diagnostic_operations.jl:56-165,480-509;
  * bulk_statistics.jl:9,87-91; moment measures polar_wavevector_grid.jl:73-115.
  * Per-(i,j) sums run n outer, m inner like the reference kernels. The total action uses a
- * Neumaier-compensated sum over (i,j). Any output pointer may be NULL. */
+ * Neumaier-compensated sum over (i,j) of m0·Δx(i)·Δy(j) with each cell's own widths. Any output
+ * pointer may be NULL. */
 void ora_diagnostics(const ora_model* M, const double* N, double* m0, double* hs, double* krms,
                      double* mean_dir, double* total_action) {
     const int64_t Nx = M->Nx, Ny = M->Ny, Nk = M->Nk, Np = M->Np;
@@ -826,7 +827,9 @@ void ora_diagnostics(const ora_model* M, const double* N, double* m0, double* hs
     if (total_action) {
         double sum = 0.0, comp = 0.0;
         for (int64_t c = 0; c < Nx * Ny; ++c) {
-            const double v = col[c] * M->dx * M->dy;
+            const double ddx = M->xspacings ? M->xspacings[c % Nx] : M->dx;
+            const double ddy = M->yspacings ? M->yspacings[c / Nx] : M->dy;
+            const double v = col[c] * ddx * ddy;   /* diagnostic_operations.jl:502: acc * Δx * Δy */
             const double tsum = sum + v;
             if (std::fabs(sum) >= std::fabs(v)) comp += (sum - tsum) + v;
             else comp += (v - tsum) + sum;

@@ -76,6 +76,9 @@ typedef struct ora_model {
     int32_t gse;
     int32_t periodic_x, periodic_y;
     double gse_alpha_s, gse_alpha_n;
+    /* per-cell widths Δx(i) (Nx) and heights Δy(j) (Ny) of the total action; NULL: dx, dy */
+    const double* xspacings;
+    const double* yspacings;
 } ora_model;
 
 /* ---- Q kernel (src/Coupling/q_kernel.jl) ---- */

@@ -3,6 +3,7 @@
 nvcc compiles every csrc/*.cu for sm_100a and links one shared library next to this
 file, so the built library travels with the source tree. Usage: python build.py [--force]
 """
+import concurrent.futures
 import os
 import shutil
 import subprocess
@@ -40,14 +41,18 @@ def build(force=False, verbose=False):
         return OUT
     objdir = os.path.join(HERE, "_build")
     os.makedirs(objdir, exist_ok=True)
-    objs = []
+    jobs = []
     for src in sources():
         obj = os.path.join(objdir, os.path.basename(src)[:-3] + ".o")
-        cmd = [NVCC, *ARCH, *FLAGS, "-c", src, "-o", obj]
-        if verbose:
+        jobs.append(([NVCC, *ARCH, *FLAGS, "-c", src, "-o", obj], obj))
+    if verbose:
+        for cmd, _ in jobs:
             print(" ".join(cmd))
-        subprocess.run(cmd, check=True)
-        objs.append(obj)
+    # one nvcc per translation unit, in parallel
+    with concurrent.futures.ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        for f in [ex.submit(subprocess.run, cmd, check=True) for cmd, _ in jobs]:
+            f.result()
+    objs = [obj for _, obj in jobs]
     cmd = [NVCC, *ARCH, "-shared", "-ccbin", "/usr/bin/g++", "-o", OUT + ".tmp", *objs]
     subprocess.run(cmd, check=True)
     os.replace(OUT + ".tmp", OUT)

@@ -76,7 +76,7 @@ void free_all(Handle* h) {
     rpl::free_currents(h);
     void* ptrs[] = {h->N, h->A, h->B, h->d_kappa, h->d_phi, h->d_cos, h->d_sin, h->d_weights, h->d_cgx,
                     h->d_cgy, h->d_cgmag, h->d_depth, h->d_coupling, h->d_wind, h->d_diag, h->d_err,
-                    h->d_coef, h->d_tab32, h->d_cell32, h->d_bin32, h->d_U};
+                    h->d_coef, h->d_tab32, h->d_cell32, h->d_bin32, h->d_U, h->d_spacing};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->h_err) cudaFreeHost(h->h_err);
@@ -206,6 +206,16 @@ int rpl_create(const rpl_desc* d, rpl_handle** out) {
     if (msg.empty()) msg = check_faces("φ", d->phi, d->phi_faces, d->Np);
     if (msg.empty() && d->kappa_faces[0] < 0.0) msg = "κ faces must be >= 0";
     if (!msg.empty()) return fail(RPL_ERR_ARGUMENT, msg);
+    if ((d->xspacings == nullptr) != (d->yspacings == nullptr))
+        return fail(RPL_ERR_ARGUMENT, "xspacings and yspacings must both be given or both be NULL");
+    if (d->xspacings) {
+        for (int64_t i = 0; i < d->Nx; ++i)
+            if (!(d->xspacings[i] > 0.0) || !std::isfinite(d->xspacings[i]))
+                return fail(RPL_ERR_ARGUMENT, "cell widths must be positive and finite");
+        for (int64_t j = 0; j < d->Ny; ++j)
+            if (!(d->yspacings[j] > 0.0) || !std::isfinite(d->yspacings[j]))
+                return fail(RPL_ERR_ARGUMENT, "cell heights must be positive and finite");
+    }
     if (d->transport != RPL_TRANSPORT_NONE) {
         if (!d->periodic_x || !d->periodic_y)
             return fail(RPL_ERR_UNSUPPORTED,
@@ -231,7 +241,7 @@ int rpl_create(const rpl_desc* d, rpl_handle** out) {
     const size_t elem = d->precision == RPL_FP64 ? 8 : 4;
     const int64_t c3 = d->Nx * d->Ny * d->Nk, P = d->Nx * d->Ny, nb = d->Nk * d->Np;
     int64_t need = 3 * units * (int64_t)elem + 16 * c3 * 8 + (d->depth_kind == RPL_DEPTH_FIELD ? (c3 + P) * 8 : 0) +
-                   (4 * P + d->Nx + d->Ny) * 8 + 6 * P * 8 + 8 * nb * 8;
+                   (4 * P + 2 * (d->Nx + d->Ny)) * 8 + 6 * P * 8 + 8 * nb * 8;
     if (d->memory_limit_bytes > 0 && need > d->memory_limit_bytes)
         return fail(RPL_ERR_OOM, "model needs " + std::to_string(need) + " device bytes, above the memory limit of " +
                                      std::to_string(d->memory_limit_bytes));
@@ -254,6 +264,11 @@ int rpl_create(const rpl_desc* d, rpl_handle** out) {
     h->kappa_faces.assign(d->kappa_faces, d->kappa_faces + d->Nk + 1);
     h->phi.assign(d->phi, d->phi + d->Np);
     h->phi_faces.assign(d->phi_faces, d->phi_faces + d->Np + 1);
+    h->spacings.resize(d->Nx + d->Ny);
+    for (int64_t i = 0; i < d->Nx; ++i) h->spacings[i] = d->xspacings ? d->xspacings[i] : d->dx;
+    for (int64_t j = 0; j < d->Ny; ++j) h->spacings[d->Nx + j] = d->yspacings ? d->yspacings[j] : d->dy;
+    h->desc.xspacings = h->spacings.data();
+    h->desc.yspacings = h->spacings.data() + d->Nx;
     if (d->depth_kind == RPL_DEPTH_FIELD) h->depth_field.assign(d->depth_field, d->depth_field + P);
     h->desc.xnodes = h->xnodes.data();
     h->desc.ynodes = h->ynodes.data();
@@ -331,6 +346,7 @@ int rpl_create(const rpl_desc* d, rpl_handle** out) {
     TRY(dalloc(h, &h->d_cgy, nb));
     TRY(dalloc(h, &h->d_wind, 4 * P + d->Nx + d->Ny));
     TRY(dalloc(h, &h->d_diag, 5 * P + 8));
+    TRY(dalloc(h, &h->d_spacing, d->Nx + d->Ny));
     TRY(dalloc(h, &h->d_err, 1));
     TRY(cudaMallocHost(&h->h_err, sizeof(unsigned int)));
     cudaStream_t s = h->stream;
@@ -343,6 +359,7 @@ int rpl_create(const rpl_desc* d, rpl_handle** out) {
     TRY(cudaMemcpyAsync(h->d_weights, tabs.data(), 4 * nb * 8, cudaMemcpyHostToDevice, s));
     TRY(cudaMemcpyAsync(h->d_cgx, cgx.data(), nb * 8, cudaMemcpyHostToDevice, s));
     TRY(cudaMemcpyAsync(h->d_cgy, cgy.data(), nb * 8, cudaMemcpyHostToDevice, s));
+    TRY(cudaMemcpyAsync(h->d_spacing, h->spacings.data(), (d->Nx + d->Ny) * 8, cudaMemcpyHostToDevice, s));
     TRY(cudaMemsetAsync(h->d_wind, 0, 4 * P * 8, s));
     TRY(cudaMemcpyAsync(h->d_wind + 4 * P, h->xnodes.data(), d->Nx * 8, cudaMemcpyHostToDevice, s));
     TRY(cudaMemcpyAsync(h->d_wind + 4 * P + d->Nx, h->ynodes.data(), d->Ny * 8, cudaMemcpyHostToDevice, s));

@@ -276,7 +276,9 @@ int rpl_ensemble_autotune(rpl_ensemble* e, int32_t force) {
     if (st) return st;
     const std::map<std::string, int> cached = read_cache(e->cache);
     std::map<std::string, std::vector<int>> classes;
-    for (size_t m = 0; m < e->members.size(); ++m) classes[e->key[m]].push_back((int)m);
+    // members with direct single-model launches never run in the persistent kernel: nothing to tune
+    for (size_t m = 0; m < e->members.size(); ++m)
+        if (!e->direct[m]) classes[e->key[m]].push_back((int)m);
     cudaEvent_t t0, t1;
     ENS_CUDA(cudaEventCreate(&t0));
     ENS_CUDA(cudaEventCreate(&t1));

@@ -96,6 +96,7 @@ constexpr TileShape kEnsembleShapes[kNumEnsembleShapes] = {
 struct Handle {
     rpl_desc desc{};
     std::vector<double> xnodes, ynodes, kappa, kappa_faces, phi, phi_faces, depth_field, weights;
+    std::vector<double> spacings;  // Nx widths then Ny heights of the cells (total action)
     int device = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
@@ -174,6 +175,7 @@ struct Handle {
     bool snap_pending = false;
     // diagnostics scratch
     double* d_diag = nullptr;      // 5 (Nx,Ny) fields + block partials
+    double* d_spacing = nullptr;   // Nx cell widths then Ny cell heights
     unsigned int* d_err = nullptr;
     unsigned int* h_err = nullptr;  // pinned
     bool force_column_kernel = false;  // RPL_FORCE_COLUMN_KERNEL=1 selects the generic FP32 column kernel

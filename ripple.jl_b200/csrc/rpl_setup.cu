@@ -351,10 +351,13 @@ diag_kernel(const T* __restrict__ N, int64_t Nx, int64_t Ny, int64_t Nk, int64_t
 }
 
 // Total action = sum_ij m0 dx dy with a compensated, deterministic two-level reduction.
-__global__ void total_kernel(const double* __restrict__ m0, int64_t P, double area, double* __restrict__ total) {
+// Total action: compensated sum over (i,j) of m0(i,j)·Δx(i)·Δy(j), each cell with its own widths
+// (diagnostic_operations.jl:492-503, bulk_statistics.jl:87-91).
+__global__ void total_kernel(const double* __restrict__ m0, int64_t Nx, int64_t P, const double* __restrict__ xsp,
+                             const double* __restrict__ ysp, double* __restrict__ total) {
     __shared__ double ss[1024], cc[1024];
     double s = 0.0, c = 0.0;
-    for (int64_t t = threadIdx.x; t < P; t += blockDim.x) kadd(s, c, m0[t] * area);
+    for (int64_t t = threadIdx.x; t < P; t += blockDim.x) kadd(s, c, m0[t] * xsp[t % Nx] * ysp[t / Nx]);
     ss[threadIdx.x] = s;
     cc[threadIdx.x] = c;
     __syncthreads();
@@ -558,7 +561,7 @@ cudaError_t launch_diagnostics(const Handle& h, const void* Nin, cudaStream_t s,
             diag_kernel<float, false><<<blocks, 256, 0, s>>>((const float*)Nin, d.Nx, d.Ny, d.Nk, d.Np, h.d_weights,
                                                              h.d_diag);
     }
-    total_kernel<<<1, 1024, 0, s>>>(h.d_diag, P, d.dx * d.dy, h.d_diag + 4 * P);
+    total_kernel<<<1, 1024, 0, s>>>(h.d_diag, d.Nx, P, h.d_spacing, h.d_spacing + d.Nx, h.d_diag + 4 * P);
     return cudaGetLastError();
 }
 

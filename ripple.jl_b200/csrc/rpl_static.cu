@@ -37,8 +37,9 @@ __device__ __forceinline__ void kadd(double& s, double& c, double v) {
     s = t;
 }
 
-// Per-(i,j) sums over the spectral bins in the order of the handle-based diagnostics, then one
-// compensated partial of m0 * dx * dy per block, written to its own slot of the scratch.
+// Per-(i,j) Kahan-compensated sums over the spectral bins (one sequential loop per column; the
+// handle-based diagnostics sum in another order, so the two agree to a few ulps, not bit for bit),
+// then one compensated partial of m0 * dx * dy per block, written to its own slot of the scratch.
 template <typename T>
 __global__ void __launch_bounds__(kColumnsPerBlock)
     static_diag_kernel(const T* __restrict__ N, int64_t P, int64_t nb, const double* __restrict__ tabs,
@@ -132,11 +133,14 @@ extern "C" int rpl_diagnostics_static(const void* N, int32_t dtype, int64_t Nx, 
     if (dtype != RPL_F64 && dtype != RPL_F32) return fail(RPL_ERR_ARGUMENT, "unknown dtype");
     if (Nx < 1 || Ny < 1 || Nk < 1 || Np < 1) return fail(RPL_ERR_ARGUMENT, "grid sizes must be positive");
     if (!(dx > 0.0) || !(dy > 0.0)) return fail(RPL_ERR_ARGUMENT, "grid spacings must be positive");
-    const int64_t P = Nx * Ny;
-    if (P > RPL_STATIC_MAX_COLUMNS)
+    // bounds checked before any product is formed, so no size can overflow into an accepted one
+    if (Nx > RPL_STATIC_MAX_COLUMNS / Ny)
         return fail(RPL_ERR_ARGUMENT, "rpl_diagnostics_static supports at most " +
                                           std::to_string((long long)RPL_STATIC_MAX_COLUMNS) +
-                                          " horizontal cells (Nx*Ny); got " + std::to_string((long long)P));
+                                          " horizontal cells (Nx*Ny); got Nx = " + std::to_string((long long)Nx) +
+                                          ", Ny = " + std::to_string((long long)Ny));
+    if (Nk > INT32_MAX / Np) return fail(RPL_ERR_ARGUMENT, "Nk*Np must stay below 2^31 spectral bins");
+    const int64_t P = Nx * Ny;
     double* partials = nullptr;
     int st = scratch_on_current_device(&partials);
     if (st) return st;

@@ -12,7 +12,7 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(os.path.dirname(_HERE), "librpl.so")
 
-RPL_ABI_VERSION = 1
+RPL_ABI_VERSION = 2
 RPL_OK, RPL_ERR_ARGUMENT, RPL_ERR_DT, RPL_ERR_NONFINITE, RPL_ERR_CUDA, RPL_ERR_OOM, \
     RPL_ERR_STATE, RPL_ERR_UNSUPPORTED, RPL_ERR_DEVICE = range(9)
 RPL_FP64, RPL_FP32 = 0, 1
@@ -38,6 +38,7 @@ class RplDesc(ctypes.Structure):
         ("kappa", _dp), ("kappa_faces", _dp), ("phi", _dp), ("phi_faces", _dp),
         ("depth_kind", _i32), ("depth_constant", _d), ("depth_field", _dp),
         ("gravity", _d), ("memory_limit_bytes", _i64),
+        ("xspacings", _dp), ("yspacings", _dp),
     ]
 
 

@@ -272,7 +272,9 @@ class SpectralWaveModel:
         lib = _lib.load()
         self._keep = dict(x=np.ascontiguousarray(grid.xnodes()), y=np.ascontiguousarray(grid.ynodes()),
                           k=spectral_grid.κ.copy(), kf=spectral_grid.κ_faces.copy(),
-                          p=spectral_grid.φ.copy(), pf=spectral_grid.φ_faces.copy())
+                          p=spectral_grid.φ.copy(), pf=spectral_grid.φ_faces.copy(),
+                          xs=np.ascontiguousarray(grid.xspacings(), dtype=np.float64),
+                          ys=np.ascontiguousarray(grid.yspacings(), dtype=np.float64))
         d = _lib.RplDesc()
         d.abi_version = _lib.RPL_ABI_VERSION
         d.precision = _lib.RPL_FP64 if precision == "fp64" else _lib.RPL_FP32
@@ -289,6 +291,7 @@ class SpectralWaveModel:
         d.depth_field = dptr(depth_field)
         d.gravity = 9.81
         d.memory_limit_bytes = int(memory_limit_bytes)
+        d.xspacings, d.yspacings = dptr(self._keep["xs"]), dptr(self._keep["ys"])
         h = _lib.ctypes.c_void_p()
         check(lib.rpl_create(_lib.ctypes.byref(d), _lib.ctypes.byref(h)))
         self._h = h

@@ -311,3 +311,78 @@ def test_error_paths():
     assert lib.rpl_step(h, 0.1, 1) == _lib.RPL_ERR_STATE
     assert lib.rpl_stage_async(h, 0.1, 4) == _lib.RPL_ERR_STATE
     assert lib.rpl_destroy(h) == _lib.RPL_OK
+
+
+def test_diagnostics_stretched_grid(oracle_mod):
+    """Total action on a stretched grid: every column weighted by its own cell area, as the oracle."""
+    from test_oracle_golden import stretched_workload
+    w = stretched_workload()
+    for precision in ("fp64", "fp32"):
+        m = w.model(precision)
+        d = rp.diagnostics(m.action)
+        do = oracle_mod.Oracle(w).diagnostics(m.action.interior().astype(np.float64))
+        assert d["total_action"] == pytest.approx(do["total_action"], rel=1e-14), precision
+        assert rel_l2(d["m0"], do["m0"]) <= 1e-14
+        m.close()
+
+
+def test_seamount_eddies_128_fp64_against_oracle(oracle_mod):
+    """The seamount-eddies physics (32 log kappa x 36 directions, 32 levels, seamount depth field, eight
+    eddies) on a 128^2 grid of the same 5120 km domain: the FP64 GPU path against the CPU oracle after
+    20 RK3 steps, rel-L2 <= 1e-12. This pins the FP64 path that the full-size FP32 comparison below
+    takes as its reference."""
+    w = workloads.seamount_eddies(N=128, Nz=32, Nk=32, Np=36, nsteps=20)
+    m, Ng, No = run_both(oracle_mod, w, 20)
+    assert rel_l2(Ng, No) <= FP64_TOL
+    d, do = rp.diagnostics(m.action), oracle_mod.Oracle(w).diagnostics(No)
+    assert rel_l2(d["Hs"], do["Hs"]) <= FP64_TOL
+    assert d["total_action"] == pytest.approx(do["total_action"], rel=FP64_TOL)
+    m.close()
+
+
+def device_state(m, precision):
+    """The model's action as a CUDA tensor in the caller layout (x fastest)."""
+    import torch
+    Nx, Ny = m.grid.Nx, m.grid.Ny
+    Nk, Np = m.spectral_grid.coordinate_size()
+    t = torch.empty(Nx * Ny * Nk * Np, dtype=torch.float64 if precision == "fp64" else torch.float32,
+                    device=f"cuda:{m.device}")
+    _lib.check(m._lib.rpl_get_action_device(m.handle, ctypes.c_void_p(t.data_ptr()),
+                                            _lib.RPL_F64 if precision == "fp64" else _lib.RPL_F32, 0))
+    return t
+
+
+def rel_l2_device(a, b, chunk=1 << 27):
+    """rel-L2 of two equal-length CUDA tensors in FP64, chunked (no full-size temporaries)."""
+    import torch
+    num = den = 0.0
+    for s in range(0, a.numel(), chunk):
+        x, y = a[s:s + chunk].double(), b[s:s + chunk].double()
+        num += float(torch.sum((x - y) ** 2))
+        den += float(torch.sum(y * y))
+    return math.sqrt(num / den)
+
+
+@pytest.mark.slow
+def test_seamount_full_run_fp32_against_fp64():
+    """The seamount-eddies configuration at full size (1024^2 x 32 levels x 32 kappa x 36 directions,
+    200 RK3 steps): the FP32 precision form against the FP64 path (pinned to the oracle above) from the
+    same initial action, rel-L2 <= 1e-5 on the action and on Hs, the total action within 1e-5, and the
+    same action-budget drift (change of the total action over the run) to 1e-5 of the total."""
+    import torch
+    w = workloads.seamount_eddies(n0_dtype=np.float32)
+    res = {}
+    for prec in ("fp64", "fp32"):
+        m = w.model(prec)
+        t0 = rp.total_action(m.action)
+        rp.time_step(m, w.dt, w.nsteps)
+        d = rp.diagnostics(m.action)
+        res[prec] = (device_state(m, prec), d["Hs"], d["total_action"], t0)
+        m.close()
+    (N32, H32, T32, S32), (N64, H64, T64, S64) = res["fp32"], res["fp64"]
+    assert rel_l2_device(N32, N64) <= FP32_TOL
+    assert rel_l2(H32, H64) <= FP32_TOL
+    assert abs(T32 - T64) <= FP32_TOL * T64
+    assert S32 == pytest.approx(S64, rel=1e-7)                       # same initial action
+    assert abs((T32 - S32) - (T64 - S64)) <= FP32_TOL * T64           # action-budget drift
+    assert float(torch.min(N32)) >= 0.0

@@ -193,3 +193,25 @@ def test_spectral_grid_defaults_match_oracle(oracle_mod):
     w = np.empty(32 * 36)
     oracle_mod.lib().ora_polar_weights(32, 36, oracle_mod.p(sg.κ_faces), oracle_mod.p(sg.φ_faces), oracle_mod.p(w))
     assert np.array_equal(sg.weights, w.reshape(32, 36, order="F"))
+
+
+def stretched_workload():
+    """A small model on a stretched horizontal grid (x faces growing geometrically, y faces ragged):
+    the total action must weight every column by its own Δx(i)·Δy(j)."""
+    xf = np.cumsum(np.concatenate([[0.0], 1.0 * 1.3 ** np.arange(9)]))
+    yf = np.array([0.0, 0.5, 2.0, 2.25, 4.0, 7.5, 8.0, 11.0])
+    g = RectilinearGrid(size=(9, 7, 2), x=xf, y=yf, z=(-1.0, 0.0))
+    sg = PolarWaveVectorGrid(κ=np.linspace(0.3, 0.9, 5), φ=np.arange(6) * 2 * math.pi / 6)
+    N0 = np.asfortranarray(np.random.default_rng(3).uniform(0.0, 1.0, (9, 7, 5, 6)))
+    return Workload("stretched", g, sg, 2.0, N0, 0.05, 1, horizontal_advection=None)
+
+
+def test_total_action_stretched_grid(oracle_mod):
+    """total_action sums density(i,j)·Δx(i)·Δy(j) per cell (diagnostic_operations.jl:492-503,
+    bulk_statistics.jl:87-91), not m0 times the first cell's area."""
+    w = stretched_workload()
+    d = oracle_mod.Oracle(w).diagnostics(w.N0)
+    dx, dy = w.grid.xspacings(), w.grid.yspacings()
+    expect = float(np.sum(d["m0"] * dx[:, None] * dy[None, :]))
+    assert d["total_action"] == pytest.approx(expect, rel=1e-14)
+    assert abs(d["total_action"] - float(np.sum(d["m0"])) * dx[0] * dy[0]) > 0.1 * expect

@@ -83,3 +83,8 @@ def test_static_diagnostics_rejects_grids_above_its_limit():
                                     None, None)
     assert st == _lib.RPL_ERR_ARGUMENT
     assert b"at most 4194304" in lib.rpl_last_error()
+    # sizes whose product wraps around in 64 bits are refused too, not accepted as a small grid
+    st = lib.rpl_diagnostics_static(p, _lib.RPL_F64, 1 << 33, 1 << 31, 1, 1, p, 1.0, 1.0, None, None, None,
+                                    None, None, None)
+    assert st == _lib.RPL_ERR_ARGUMENT
+    assert b"at most 4194304" in lib.rpl_last_error()
