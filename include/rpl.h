@@ -168,6 +168,39 @@ int rpl_set_sources(rpl_handle* h, const rpl_sources* s);
 /* Host-evaluated wind (any wind struct of src/Forcing/winds.jl) for RPL_WIND_FIELD: (Nx,Ny) arrays. */
 int rpl_set_wind_field(rpl_handle* h, const double* U10, const double* direction);
 
+/* Source terms of a SourceTermSet (src/Sources/Sources.jl:5-11,443-449) whose tendency is linear in the
+ * action: each adds positive - damping * N with (positive, damping) from split_growth_rate (wind input)
+ * or split_damping_rate (dissipation) of its rate (Sources.jl:430-434). */
+typedef enum rpl_term_kind {
+    RPL_TERM_EXPONENTIAL_WIND = 1, /* ExponentialWindInput (Sources.jl:32-39,492-496): rate times the cell
+                                      average of max(cos(phi - direction), 0)^p[0], p[0] a nonnegative integer */
+    RPL_TERM_WAVE_AGE_WIND = 2,    /* WaveAgeWindInput (Sources.jl:67-95,522-554): p = (inverse wave-age
+                                      threshold, power, spreading power), gravity */
+    RPL_TERM_WHITECAPPING = 3,     /* WhitecappingDissipation (Sources.jl:105-122,583-598): p = (saturation
+                                      threshold, saturation power, wavenumber power, reference wavenumber) */
+    RPL_TERM_MEAN_SPECTRUM = 4     /* MeanSpectrumWhitecapping (mean_spectrum.jl:20-111): p = (C_ds, delta1,
+                                      delta2, mean exponent), gravity */
+} rpl_term_kind;
+#define RPL_MAX_TERMS 8
+
+typedef struct rpl_source_term {
+    int32_t kind;               /* rpl_term_kind */
+    int32_t reserved;
+    double rate;                /* a Number rate, or rate_field (Nx,Ny, x fastest) when not NULL */
+    const double* rate_field;
+    double direction;           /* wind direction of the wind-input terms */
+    double speed;               /* WaveAgeWindInput speed, or speed_field (Nx,Ny) when not NULL */
+    const double* speed_field;
+    double p[4];                /* per kind, see rpl_term_kind */
+    double gravity;
+} rpl_source_term;
+
+/* Replaces sources=SourceTermSet(terms...) (or one such term) on this path: up to RPL_MAX_TERMS terms,
+ * evaluated on the device before every stage (per-(i,j) moments by a warp per column, then a rate per
+ * cell-bin) and applied inside the stage kernels; count = 0 removes them. May be combined with
+ * rpl_set_sources (the bundle's tendency comes first). Fields are copied. */
+int rpl_set_source_terms(rpl_handle* h, const rpl_source_term* terms, int32_t count);
+
 /* Replaces set!(model, N=array) / set!(::ProductField, ::AbstractArray) (set.jl:20-30,44-48). */
 int rpl_set_action(rpl_handle* h, const void* N, int32_t dtype, int32_t layout);
 /* Replaces interior(model.action) (product_field.jl:232-235). */
@@ -348,6 +381,12 @@ int rpl_mlp_forward(rpl_mlp* m, const void* X, const float* E, int64_t n, float*
 /* The tensor-core GEMM alone (for testing): C (M x N FP32) = A (M x K BF16) * B (N x K BF16)^T, device
  * row-major arrays, M % 128 == 0, N % 128 == 0, K % 64 == 0; stream NULL = default. */
 int rpl_gemm_bf16(const void* A, const void* B, float* C, int32_t M, int32_t N, int32_t K, void* stream);
+/* rpl_gemm_bf16 with every barrier wait bounded by `wait_limit` polls (0: the default, 2^24). A wait that
+ * runs out ends the kernel cleanly (loads and MMAs in flight drained, tensor memory freed) and the call
+ * returns RPL_ERR_DEVICE; the context stays usable. No counterpart in the reference: it lets a caller
+ * (or a test) check the abort path of the tensor-core kernels without a device fault. */
+int rpl_gemm_bf16_bounded(const void* A, const void* B, float* C, int32_t M, int32_t N, int32_t K,
+                          uint32_t wait_limit, void* stream);
 /* Training pairs of the FP32 handle's current state and clock from its plain sources: for every cell c
  * (c = i + Nx j) row c of X, E and T (device arrays of Nx*Ny rows; T = asinh(rate / target_scale)). */
 int rpl_learned_sample(rpl_handle* h, const rpl_mlp* m, void* X, float* E, float* T);

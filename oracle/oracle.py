@@ -29,6 +29,11 @@ class OraHolland(ctypes.Structure):
                 ("track_t", _dp), ("center_x", _dp), ("center_y", _dp)]
 
 
+class OraTerm(ctypes.Structure):
+    _fields_ = [("kind", _i32), ("pad", _i32), ("rate", _d), ("rate_field", _dp), ("direction", _d), ("speed", _d),
+                ("speed_field", _dp), ("p", _d * 4), ("gravity", _d)]
+
+
 class OraModel(ctypes.Structure):
     _fields_ = [("Nx", _i64), ("Ny", _i64), ("Nk", _i64), ("Np", _i64), ("dx", _d), ("dy", _d),
                 ("xnodes", _dp), ("ynodes", _dp), ("kappa", _dp), ("kappa_faces", _dp), ("phi", _dp),
@@ -41,7 +46,7 @@ class OraModel(ctypes.Structure):
                 ("ds_p", _d), ("sigma_power", _d), ("ds_gravity", _d), ("pm_mode", _i32), ("pm_per_cell", _i32),
                 ("pm_overlap", _dp), ("pm_kx", _dp), ("pm_ky", _dp), ("gse", _i32), ("periodic_x", _i32),
                 ("periodic_y", _i32), ("gse_alpha_s", _d), ("gse_alpha_n", _d), ("xspacings", _dp),
-                ("yspacings", _dp)]
+                ("yspacings", _dp), ("n_terms", _i32), ("terms", ctypes.POINTER(OraTerm))]
 
 
 def build():
@@ -322,7 +327,26 @@ class Oracle:
         m = self.m
         m.wind_kind = WIND_NONE
         m.has_dissipation = 0
+        m.n_terms = 0
         if s is None:
+            return
+        from ripple_b200.sources import linear_terms, term_record
+        terms = linear_terms(s)
+        if terms is not None:
+            arr = (OraTerm * max(1, len(terms)))()
+            for k, t in enumerate(terms):
+                kind, rate, rf, direction, speed, sf, prm, grav = term_record(t, self.w.grid)
+                arr[k].kind, arr[k].rate, arr[k].direction, arr[k].speed, arr[k].gravity = kind, rate, direction, speed, grav
+                for q in range(4):
+                    arr[k].p[q] = prm[q]
+                if rf is not None:
+                    self._keep.append(rf)
+                    arr[k].rate_field = p(rf)
+                if sf is not None:
+                    self._keep.append(sf)
+                    arr[k].speed_field = p(sf)
+            self._keep.append(arr)
+            m.n_terms, m.terms = len(terms), arr
             return
         name = type(s).__name__
         wind_input = dissipation = None

@@ -671,6 +671,146 @@ static void add_sources(const ora_model* M, const double* N, double t, double* G
         }
 }
 
+/* ------------------------------------------------------ SourceTermSet terms */
+
+/* Sources.jl:1394-1400 */
+static double cosine_power_antiderivative(double a, int power) {
+    if (power == 0) return a;
+    if (power == 1) return std::sin(a);
+    return std::sin(a) * std::pow(std::cos(a), power - 1) / power +
+           (double)(power - 1) / power * cosine_power_antiderivative(a, power - 2);
+}
+
+/* Sources.jl:1402-1421: integral of max(cos, 0)^power over [a1, a2] */
+double ora_positive_cosine_power_integral(double a1, double a2, int power) {
+    if (a2 < a1) return -ora_positive_cosine_power_integral(a2, a1, power);
+    if (power == 0) return a2 - a1;
+    const double period = 2.0 * M_PI;
+    const int64_t lo = (int64_t)std::floor((a1 - M_PI / 2) / period) - 1;
+    const int64_t hi = (int64_t)std::ceil((a2 + M_PI / 2) / period) + 1;
+    double integral = 0.0;
+    for (int64_t q = lo; q <= hi; ++q) {
+        const double shift = q * period;
+        const double left = std::max(a1, shift - M_PI / 2), right = std::min(a2, shift + M_PI / 2);
+        if (!(right > left)) continue;
+        integral += cosine_power_antiderivative(right - shift, power) - cosine_power_antiderivative(left - shift, power);
+    }
+    return integral;
+}
+
+/* Sources.jl:1423-1434 (polar grid): the cell average of max(cos(phi - direction), 0)^power */
+double ora_wind_directional_weight(const ora_model* M, int64_t n, double direction, int power) {
+    if (power == 0) return 1.0;
+    const double p1 = M->phi_faces[n], p2 = M->phi_faces[n + 1];
+    return ora_positive_cosine_power_integral(p1 - direction, p2 - direction, power) / (p2 - p1);
+}
+
+/* finite_volume_integration.jl:24-27,29-33,86-88: radial-power average kappa^power over the cell */
+double ora_radial_power_average(const ora_model* M, int64_t m, int64_t n, double power) {
+    const double k1 = M->kappa_faces[m], k2 = M->kappa_faces[m + 1];
+    const double p1 = M->phi_faces[n], p2 = M->phi_faces[n + 1];
+    const double meas = (p2 - p1) * (std::pow(k2, power + 2.0) - std::pow(k1, power + 2.0)) / (power + 2.0);
+    return meas / M->weights[m + M->Nk * n];
+}
+
+static double term_value(double v, const double* field, int64_t c) { return field ? field[c] : v; }
+
+/* Source tendency of the SourceTermSet terms added to G (tendencies.jl:34-36: G += source_tendency; the
+ * set sums its terms in order, Sources.jl:443-449). Per-(i,j) integrals as the reference computes them
+ * per call: local_zeroth_moment (Sources.jl:1471-1480, n outer m inner, every bin), and for
+ * MeanSpectrumWhitecapping the p-th means over bins with N > 0 and k > 0 (mean_spectrum.jl:43-82). */
+static void add_source_terms(const ora_model* M, const double* N, double* G) {
+    const int64_t Nx = M->Nx, Ny = M->Ny, Nk = M->Nk, Np = M->Np, P = Nx * Ny;
+#pragma omp parallel for schedule(static)
+    for (int64_t c = 0; c < P; ++c) {
+        // per-(i,j) integrals
+        double m0 = 0.0;
+        for (int64_t n = 0; n < Np; ++n)
+            for (int64_t m = 0; m < Nk; ++m) m0 += N[c + P * (m + Nk * n)] * M->weights[m + Nk * n];
+        std::vector<double> kbar(M->n_terms, 0.0), sbar(M->n_terms, 0.0);
+        for (int32_t t = 0; t < M->n_terms; ++t) {
+            const ora_term& T = M->terms[t];
+            if (T.kind != ORA_TERM_MEAN_SPECTRUM) continue;
+            const double p = T.p[3];
+            double nk = 0.0, dk = 0.0, ns = 0.0, ds = 0.0;
+            for (int64_t n = 0; n < Np; ++n)
+                for (int64_t m = 0; m < Nk; ++m) {
+                    const double a = N[c + P * (m + Nk * n)];
+                    if (a <= 0.0) continue;
+                    const double w = M->weights[m + Nk * n];
+                    const double kx = M->kappa[m] * std::cos(M->phi[n]), ky = M->kappa[m] * std::sin(M->phi[n]);
+                    const double k = std::hypot(kx, ky);
+                    if (k <= 0.0) continue;
+                    nk += a * w * std::pow(k, p);
+                    dk += a * w;
+                    ns += a * w * std::pow(std::sqrt(T.gravity * k), p);
+                    ds += a * w;
+                }
+            kbar[t] = dk > 0.0 ? std::pow(nk / dk, 1.0 / p) : 0.0;
+            sbar[t] = ds > 0.0 ? std::pow(ns / ds, 1.0 / p) : 0.0;
+        }
+        for (int64_t n = 0; n < Np; ++n)
+            for (int64_t m = 0; m < Nk; ++m) {
+                const int64_t u = c + P * (m + Nk * n);
+                const double a = N[u];
+                const double kx = M->kappa[m] * std::cos(M->phi[n]), ky = M->kappa[m] * std::sin(M->phi[n]);
+                const double k = std::hypot(kx, ky);
+                double total = 0.0;
+                for (int32_t t = 0; t < M->n_terms; ++t) {
+                    const ora_term& T = M->terms[t];
+                    double positive = 0.0, damping = 0.0;
+                    bool growth = true;   // split_growth_rate of `rate`, else split_damping_rate
+                    double rate = 0.0;
+                    switch (T.kind) {
+                        case ORA_TERM_EXPONENTIAL_WIND:  // Sources.jl:492-496
+                            rate = term_value(T.rate, T.rate_field, c) *
+                                   ora_wind_directional_weight(M, n, T.direction, (int)T.p[0]);
+                            break;
+                        case ORA_TERM_WAVE_AGE_WIND: {  // Sources.jl:522-554
+                            const double kr = M->kappa[m];   // radial_wavenumber (polar_wavevector_grid.jl:70)
+                            if (kr <= 0.0) break;
+                            const double al =
+                                k == 0.0 ? 0.0 : std::max((kx * std::cos(T.direction) + ky * std::sin(T.direction)) / k, 0.0);
+                            if (al == 0.0) break;
+                            const double speed = term_value(T.speed, T.speed_field, c);
+                            const double inv_age = speed * al / std::sqrt(T.gravity / kr);
+                            const double excess = std::max(inv_age - T.p[0], 0.0);
+                            rate = term_value(T.rate, T.rate_field, c) * std::pow(excess, T.p[1]) * std::pow(al, T.p[2]);
+                            break;
+                        }
+                        case ORA_TERM_WHITECAPPING: {  // Sources.jl:588-598, 568-573
+                            growth = false;
+                            const double excess = std::max(m0 / T.p[0] - 1.0, 0.0);
+                            const double weighting = T.p[2] == 0.0 ? 1.0
+                                                                   : ora_radial_power_average(M, m, n, T.p[2]) /
+                                                                         std::pow(T.p[3], T.p[2]);
+                            rate = term_value(T.rate, T.rate_field, c) * std::pow(excess, T.p[1]) * weighting;
+                            break;
+                        }
+                        case ORA_TERM_MEAN_SPECTRUM: {  // mean_spectrum.jl:90-111
+                            growth = false;
+                            if (!(m0 > 0.0) || !(kbar[t] > 0.0) || !(k > 0.0)) break;
+                            const double alpha = m0 * kbar[t] * kbar[t];
+                            const double ratio = k / kbar[t];
+                            const double bracket = T.p[1] * ratio + T.p[2] * ratio * ratio;
+                            rate = -T.p[0] * alpha * alpha * sbar[t] * bracket;
+                            break;
+                        }
+                        default:
+                            break;
+                    }
+                    if (growth) {
+                        if (rate >= 0.0) positive = rate * a; else damping = -rate;
+                    } else {
+                        if (rate >= 0.0) damping = rate; else positive = -rate * a;
+                    }
+                    total += positive - damping * a;
+                }
+                G[u] += total;
+            }
+    }
+}
+
 /* src/Models/tendencies.jl:28-41,82-101 (dispatch) */
 void ora_tendency(const ora_model* M, const double* N, double t, int32_t with_sources, double* G) {
     const int64_t total = M->Nx * M->Ny * M->Nk * M->Np;
@@ -696,6 +836,7 @@ void ora_tendency(const ora_model* M, const double* N, double t, int32_t with_so
     else if (M->transport == ORA_TRANSPORT_INTRINSIC) intrinsic_tendency(M, N, G);
     else std::memset(G, 0, sizeof(double) * total);
     if (with_sources && (M->wind_kind != ORA_WIND_NONE || M->has_dissipation)) add_sources(M, N, t, G);
+    if (with_sources && M->n_terms > 0) add_source_terms(M, N, G);
 }
 
 /* src/Models/propagation_smoothing.jl:60-109 (_spatial_averaging_kernel!), :117-158 (tables),

@@ -38,6 +38,32 @@ typedef struct ora_holland {
     const double* center_y;
 } ora_holland;
 
+/* Source terms of a SourceTermSet (src/Sources/Sources.jl:5-11,443-449) whose tendency is linear in the
+ * action: positive - damping * N with (positive, damping) from split_growth_rate / split_damping_rate
+ * (Sources.jl:430-434). */
+enum {
+    ORA_TERM_EXPONENTIAL_WIND = 1, /* ExponentialWindInput (Sources.jl:32-39,492-501): p[0] spreading power */
+    ORA_TERM_WAVE_AGE_WIND = 2,    /* WaveAgeWindInput (Sources.jl:67-95,522-559): p[0] inverse wave-age
+                                      threshold, p[1] power, p[2] spreading power, gravity */
+    ORA_TERM_WHITECAPPING = 3,     /* WhitecappingDissipation (Sources.jl:105-122,583-598): p[0] saturation
+                                      threshold, p[1] saturation power, p[2] wavenumber power,
+                                      p[3] reference wavenumber */
+    ORA_TERM_MEAN_SPECTRUM = 4     /* MeanSpectrumWhitecapping (mean_spectrum.jl:20-115): p[0] C_ds,
+                                      p[1] delta1, p[2] delta2, p[3] p, gravity */
+};
+
+typedef struct ora_term {
+    int32_t kind;
+    int32_t pad;
+    double rate;                /* source_value of a Number; rate_field (Nx,Ny) x fastest when not NULL */
+    const double* rate_field;
+    double direction;           /* wind direction of the wind-input terms (a Number) */
+    double speed;               /* WaveAgeWindInput speed; speed_field (Nx,Ny) when not NULL */
+    const double* speed_field;
+    double p[4];
+    double gravity;
+} ora_term;
+
 typedef struct ora_model {
     int64_t Nx, Ny, Nk, Np;
     double dx, dy;                       /* first(xspacings), first(yspacings) */
@@ -79,6 +105,9 @@ typedef struct ora_model {
     /* per-cell widths Δx(i) (Nx) and heights Δy(j) (Ny) of the total action; NULL: dx, dy */
     const double* xspacings;
     const double* yspacings;
+    /* SourceTermSet terms, applied after the bundle above (both may be present) */
+    int32_t n_terms;
+    const ora_term* terms;
 } ora_model;
 
 /* ---- Q kernel (src/Coupling/q_kernel.jl) ---- */

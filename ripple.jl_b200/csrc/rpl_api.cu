@@ -70,6 +70,7 @@ cudaError_t dalloc(Handle* h, T** p, size_t count) {
 
 void free_all(Handle* h) {
     rpl::free_output(h);
+    rpl::free_terms(h);
     rpl::free_smooth(h);
     rpl::free_learned(h);
     rpl::free_pm(h);
@@ -152,6 +153,7 @@ int launch_step(Handle* h, double dt, int stage_only) {
             else if (h->src.stress_cap) RPL_CUDA(rpl::launch_stress_factor(*h, Nin, s));
         }
         if (h->pm) RPL_CUDA(rpl::launch_pm_refresh(*h, Nin, s, false));
+        if (h->n_terms) RPL_CUDA(rpl::launch_terms(*h, Nin, s));
         const rpl::StageParams p = rpl::make_params(*h, dt, stage);
         RPL_CUDA(rpl::launch_stage(*h, p, Nin, h->N, Nout, s));
         if (stage == 3 && h->smooth) RPL_CUDA(rpl::launch_smooth(*h, h->A, h->N, dt, s));  // time_step.jl:168
@@ -827,6 +829,7 @@ int rpl_tendency(rpl_handle* hh, double* G, int32_t layout) {
         if (e == cudaSuccess && h->src.stress_cap) e = rpl::launch_stress_factor(*h, h->N, s);
     }
     if (e == cudaSuccess && h->pm) e = rpl::launch_pm_refresh(*h, h->N, s, true);
+    if (e == cudaSuccess && h->n_terms) e = rpl::launch_terms(*h, h->N, s);
     if (e == cudaSuccess) e = rpl::launch_tendency(*h, rpl::make_params(*h, 1.0, 1), h->N, dG, s);
     if (e == cudaSuccess)
         e = rpl::launch_from_device_layout(*h, dG, RPL_F64, dGx, RPL_F64, 0, h->desc.Np, 0, h->desc.Nk, s);

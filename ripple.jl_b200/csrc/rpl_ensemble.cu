@@ -357,7 +357,7 @@ int rpl_ensemble_create(rpl_handle* const* members, const double* dt, int32_t co
                          who + "ensembles take FP32 models with 4 <= Nk <= 32, Nk % 4 == 0, Nx, Ny >= 3 and transport");
         if (h.desc.transport != h0.desc.transport)
             return efail(RPL_ERR_UNSUPPORTED, who + "members must share one transport kind");
-        if (h.has_sources) return efail(RPL_ERR_UNSUPPORTED, who + "ensemble members carry no sources");
+        if (h.has_sources || h.n_terms) return efail(RPL_ERR_UNSUPPORTED, who + "ensemble members carry no sources");
         if (h.desc.transport == RPL_TRANSPORT_REFRACTION && !h.currents_set)
             return efail(RPL_ERR_STATE, who + "refraction transport needs rpl_set_currents first");
         if (h.pm)

@@ -14,9 +14,11 @@
 //     wait `acc_full`, read their lanes with tcgen05.ld, apply the fused epilogue, store, and arrive on
 //     `acc_empty` so the MMA warp may reuse that accumulator -- the epilogue of one tile overlaps the
 //     MMAs of the next.
-// Every wait is bounded and checks a shared abort flag: a wait that gives up sets bit 4 of the error word
-// and the flag, every role then leaves its loop, the copies in flight drain, TMEM is freed, and the
-// kernel returns. Requirements (checked by the host): M % 128 == 0, N % BN == 0, K % 64 == 0, 16-byte
+// Every wait is bounded (GemmArgs::wait_limit polls, default 2^24) and checks a shared abort flag: a wait
+// that gives up sets bit 4 of the error word and the flag, every role then leaves its loop; the producer
+// waits (bounded) for the TMA loads it issued to land and the MMA thread for its issued MMAs to finish,
+// so nothing writes shared or tensor memory after the CTA frees them; then TMEM is freed and the kernel
+// returns. Requirements (checked by the host): M % 128 == 0, N % BN == 0, K % 64 == 0, 16-byte
 // aligned rows.
 #include <cuda.h>
 #include <cuda_bf16.h>
@@ -36,7 +38,8 @@ constexpr int MMA_WARP = 1;
 constexpr int EPI_WARP0 = 2, EPI_WARPS = 16;   // warps 2-17
 constexpr int EPILOGUE = EPI_WARPS * 32;
 constexpr int THREADS = (EPI_WARP0 + EPI_WARPS) * 32;
-constexpr uint32_t WAIT_LIMIT = 1u << 24;
+constexpr uint32_t WAIT_LIMIT = 1u << 24;   // default polls per barrier wait
+constexpr uint32_t DRAIN_LIMIT = 1u << 24;  // polls per wait for work in flight after an abort
 
 template <int BN>
 struct GemmSmem {
@@ -68,9 +71,9 @@ __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 
-// Bounded wait that also gives up once another role has aborted.
-__device__ __forceinline__ bool wait_phase(uint32_t bar, uint32_t parity, volatile int* abort_flag) {
-    for (uint32_t i = 0; i < WAIT_LIMIT; ++i) {
+// Bounded wait (`limit` polls) that also gives up once another role has aborted.
+__device__ __forceinline__ bool wait_phase(uint32_t bar, uint32_t parity, volatile int* abort_flag, uint32_t limit) {
+    for (uint32_t i = 0; i < limit; ++i) {
         if (umma::mbar_try_wait(bar, parity)) return true;
         if (*abort_flag) return false;
     }
@@ -157,7 +160,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, const GemmArgs g) {
     using S = GemmSmem<BN>;
     extern __shared__ uint8_t smem_raw[];
-    __shared__ uint64_t full_bar[STAGES], empty_bar[STAGES], acc_full[2], acc_empty[2];
+    __shared__ uint64_t full_bar[STAGES], empty_bar[STAGES], acc_full[2], acc_empty[2], drain_bar;
     __shared__ uint32_t s_tmem;
     __shared__ int s_abort;
     volatile int* abort_flag = &s_abort;
@@ -165,6 +168,10 @@ __global__ void __launch_bounds__(THREADS, 1)
     const int tiles_n = g.N / BN, tiles = (g.M / BM) * tiles_n;
     const int KB = g.K / BK;
     const uint32_t base = (umma::smem_u32(smem_raw) + 1023u) & ~1023u;
+    const uint32_t limit = g.wait_limit ? g.wait_limit : WAIT_LIMIT;
+    int64_t last_use[STAGES];  // producer thread: per stage, the fill count of its last issued load (-1: none)
+#pragma unroll
+    for (int q = 0; q < STAGES; ++q) last_use[q] = -1;
 
     if (tid == 0) {
         for (int s = 0; s < STAGES; ++s) {
@@ -175,6 +182,7 @@ __global__ void __launch_bounds__(THREADS, 1)
             umma::mbar_init(umma::smem_u32(&acc_full[b]), 1);
             umma::mbar_init(umma::smem_u32(&acc_empty[b]), EPILOGUE);
         }
+        umma::mbar_init(umma::smem_u32(&drain_bar), 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         s_abort = 0;
     }
@@ -194,13 +202,16 @@ __global__ void __launch_bounds__(THREADS, 1)
                     const int s = (int)(gcount % STAGES);
                     const int64_t use = gcount / STAGES;
                     if (use > 0 &&
-                        !wait_phase(umma::smem_u32(&empty_bar[s]), (uint32_t)((use - 1) & 1), abort_flag))
+                        !wait_phase(umma::smem_u32(&empty_bar[s]), (uint32_t)((use - 1) & 1), abort_flag, limit))
                         break;
                     const uint32_t sa = base + s * S::STAGE, sb = sa + S::A_BYTES;
                     const uint32_t bar = umma::smem_u32(&full_bar[s]);
                     umma::mbar_arrive_expect_tx(bar, (uint32_t)S::STAGE);
                     umma::tma_load_2d(sa, &tmA, kb * BK, m0, bar);
                     umma::tma_load_2d(sb, &tmB, kb * BK, n0, bar);
+#pragma unroll
+                    for (int q = 0; q < STAGES; ++q)
+                        if (q == s) last_use[q] = use;
                 }
             }
         }
@@ -213,13 +224,13 @@ __global__ void __launch_bounds__(THREADS, 1)
             int local = 0;
             for (int t = blockIdx.x; t < tiles && !*abort_flag; t += gridDim.x, ++local) {
                 const int b = local & 1, ub = local >> 1;
-                if (ub > 0 && !wait_phase(umma::smem_u32(&acc_empty[b]), (uint32_t)((ub - 1) & 1), abort_flag)) break;
+                if (ub > 0 && !wait_phase(umma::smem_u32(&acc_empty[b]), (uint32_t)((ub - 1) & 1), abort_flag, limit)) break;
                 umma::fence_after_sync();
                 const uint32_t acc = tmem + (uint32_t)(b * BN);
                 bool ok = true;
                 for (int kb = 0; kb < KB; ++kb, ++gcount) {
                     const int s = (int)(gcount % STAGES);
-                    if (!wait_phase(umma::smem_u32(&full_bar[s]), (uint32_t)((gcount / STAGES) & 1), abort_flag)) {
+                    if (!wait_phase(umma::smem_u32(&full_bar[s]), (uint32_t)((gcount / STAGES) & 1), abort_flag, limit)) {
                         ok = false;
                         break;
                     }
@@ -242,7 +253,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         int local = 0;
         for (int t = blockIdx.x; t < tiles && !*abort_flag; t += gridDim.x, ++local) {
             const int b = local & 1;
-            if (!wait_phase(umma::smem_u32(&acc_full[b]), (uint32_t)((local >> 1) & 1), abort_flag)) break;
+            if (!wait_phase(umma::smem_u32(&acc_full[b]), (uint32_t)((local >> 1) & 1), abort_flag, limit)) break;
             umma::fence_after_sync();
             const int m0 = (t / tiles_n) * BM, n0 = (t % tiles_n) * BN;
             const uint32_t trow = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(b * BN + part * (BN / 4));
@@ -251,7 +262,23 @@ __global__ void __launch_bounds__(THREADS, 1)
             mbar_arrive(umma::smem_u32(&acc_empty[b]));
         }
     }
-    if (tid == 0 && *abort_flag && g.err) atomicOr(g.err, 4u);
+    umma::fence_before_sync();
+    __syncthreads();  // every role has left its loop; the abort flag is final
+    if (*abort_flag) {
+        if (warp == 0 && lane == 0) {
+            // every TMA load still in flight lands before the CTA releases its shared memory
+#pragma unroll
+            for (int q = 0; q < STAGES; ++q)
+                if (last_use[q] >= 0)
+                    umma::mbar_wait_bounded(umma::smem_u32(&full_bar[q]), (uint32_t)(last_use[q] & 1), DRAIN_LIMIT);
+        }
+        if (warp == MMA_WARP && lane == 0) {
+            // every MMA issued so far (and its barrier arrivals) completes before TMEM is freed
+            umma::mma_commit(umma::smem_u32(&drain_bar));
+            umma::mbar_wait_bounded(umma::smem_u32(&drain_bar), 0u, DRAIN_LIMIT);
+        }
+        if (tid == 0 && g.err) atomicOr(g.err, 4u);
+    }
     umma::fence_before_sync();
     __syncthreads();
     if (warp == MMA_WARP) {

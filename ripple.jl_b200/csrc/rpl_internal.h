@@ -56,6 +56,7 @@ struct StageParams {
     double C_ds, B_r, ds_p, sigma_power, ds_g;
     float wind_K32, von_karman32, z_alpha32;  // FP32 copies: rho_ratio beta_max / kappa_vk^2, kappa_vk, z_alpha
     unsigned int* err;                      // device error word
+    const void* lin_rates;                  // SourceTermSet rates per cell-bin (state layout and type) or null
 };
 
 // Arguments of one FP32 tile-kernel stage launch over one model (rpl_tile32.cu): the buffers and the
@@ -79,6 +80,7 @@ struct TileArgs {
     const float* lrate;
     const unsigned int* lflag;
     int learned, pad1;
+    const float* lin_rates;  // SourceTermSet rates per cell-bin (state layout) or null
 };
 
 // Tile shapes (kappa-pair lanes per cell L, tile TX x TY) compiled into the ensemble kernel; every
@@ -173,6 +175,12 @@ struct Handle {
     void* d_snap = nullptr;              // staging buffer, caller layout
     int64_t snap_bytes = 0;
     bool snap_pending = false;
+    // SourceTermSet terms (rpl_terms.cu)
+    int n_terms = 0;
+    rpl_source_term terms[RPL_MAX_TERMS] = {};  // field pointers refer to d_terms_fields
+    void* d_lin_rates = nullptr;   // per cell-bin rate, state layout and type
+    double* d_terms = nullptr;     // per term 3 bin tables (Nk*Np each) then the copied fields
+    int64_t terms_bytes = 0;
     // diagnostics scratch
     double* d_diag = nullptr;      // 5 (Nx,Ny) fields + block partials
     double* d_spacing = nullptr;   // Nx cell widths then Ny cell heights
@@ -204,6 +212,10 @@ void free_output(Handle* h);
 // SpatialAveraging of the state Nin into Nout with the step's dt; release of its tables (rpl_smooth.cu).
 cudaError_t launch_smooth(Handle& h, const void* Nin, void* Nout, double dt, cudaStream_t s);
 void free_smooth(Handle* h);
+
+// SourceTermSet rates of the action Nin into d_lin_rates; release of their buffers (rpl_terms.cu).
+cudaError_t launch_terms(const Handle& h, const void* Nin, cudaStream_t s);
+void free_terms(Handle* h);
 
 // Sets the thread-local message rpl_last_error() returns (rpl_api.cu).
 void set_last_error(const std::string& msg);

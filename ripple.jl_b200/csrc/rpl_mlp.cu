@@ -526,9 +526,15 @@ int rpl_mlp_forward(rpl_mlp* m, const void* X, const float* E, int64_t n, float*
 }
 
 int rpl_gemm_bf16(const void* A, const void* B, float* C, int32_t M, int32_t N, int32_t K, void* stream) {
+    return rpl_gemm_bf16_bounded(A, B, C, M, N, K, 0u, stream);
+}
+
+int rpl_gemm_bf16_bounded(const void* A, const void* B, float* C, int32_t M, int32_t N, int32_t K,
+                          uint32_t wait_limit, void* stream) {
     rpl::GemmArgs g{};
     g.A = (const bf16*)A; g.lda = K; g.B = (const bf16*)B; g.ldb = K; g.M = M; g.N = N; g.K = K;
     g.epi = rpl::EPI_F32; g.out_f32 = C; g.ldo = N;
+    g.wait_limit = wait_limit;
     const int bn = (N % 256 == 0 && (M / 128) * (N / 256) >= 148) ? 256 : 128;
     if (!rpl::gemm_shape_ok(g, bn)) return mfail(RPL_ERR_ARGUMENT, "GEMM shape or alignment not supported");
     unsigned int* err = nullptr;
@@ -542,7 +548,7 @@ int rpl_gemm_bf16(const void* A, const void* B, float* C, int32_t M, int32_t N, 
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     cudaFree(err);
     if (e != cudaSuccess) return mcuda(e, "rpl_gemm_bf16");
-    if (w) return mfail(RPL_ERR_DEVICE, "the GEMM gave up waiting for its MMAs");
+    if (w) return mfail(RPL_ERR_DEVICE, "the GEMM gave up waiting on a barrier (bounded wait ran out)");
     return RPL_OK;
 }
 

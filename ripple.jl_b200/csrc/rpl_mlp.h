@@ -37,6 +37,7 @@ struct GemmArgs {
     const float* clamp_lo;   // EPI_BIAS: per-column bounds the output is clamped to (both or neither)
     const float* clamp_hi;
     unsigned int* err;       // bit 4: a bounded wait gave up
+    uint32_t wait_limit;     // polls before a barrier wait gives up; 0: the kernel's default
 };
 
 bool gemm_shape_ok(const GemmArgs& g, int bn);

@@ -282,6 +282,7 @@ __global__ void __launch_bounds__(BLOCK) column_kernel(const T* __restrict__ Nin
             G = -(fx + fy);
         }
         if (p.has_wind || p.has_diss) G = G + T(source_term(p, cc, mm, n, (double)c0));
+        if (p.lin_rates) G = fma(static_cast<const T*>(p.lin_rates)[at], c0, G);
         if constexpr (TENDENCY) {
             if (live) Gout[at] = (double)G;
         } else {
@@ -339,6 +340,7 @@ __global__ void __launch_bounds__(BLOCK) generic_kernel(const T* __restrict__ Ni
         G = -(fx + fy);
     }
     if (p.has_wind || p.has_diss) G = G + T(source_term(p, c, m, n, (double)c0));
+    if (p.lin_rates) G = fma(static_cast<const T*>(p.lin_rates)[t], c0, G);
     if constexpr (TENDENCY) {
         Gout[t] = (double)G;
     } else {
@@ -361,6 +363,7 @@ __global__ void __launch_bounds__(BLOCK) source_only_kernel(const T* __restrict_
     const T a = Nin[t];
     T G = T(0);
     if (p.has_wind || p.has_diss) G = T(source_term(p, cn % P, m, (int)(cn / P), (double)a));
+    if (p.lin_rates) G = fma(static_cast<const T*>(p.lin_rates)[t], a, G);
     if constexpr (TENDENCY) {
         Gout[t] = (double)G;
     } else {
@@ -447,13 +450,16 @@ StageParams make_params(const Handle& h, double dt, int stage) {
     p.von_karman32 = (float)p.von_karman;
     p.z_alpha32 = (float)p.z_alpha;
     p.err = h.d_err;
+    p.lin_rates = h.n_terms ? h.d_lin_rates : nullptr;
     return p;
 }
 
 cudaError_t launch_stage(const Handle& h, const StageParams& p, const void* Nin, const void* N0, void* Nout,
                          cudaStream_t s) {
     if (h.precision == RPL_FP64) return launch_impl<double, false>(h, p, Nin, N0, Nout, nullptr, s);
-    if (tile32_supported(h) && !h.force_column_kernel) return launch_tile32(h, p, Nin, N0, Nout, s);
+    // the tile kernel takes the SourceTermSet rates alone, not together with the bundle or the network
+    const bool mixed = p.lin_rates && (p.has_wind || p.has_diss || p.learned);
+    if (tile32_supported(h) && !h.force_column_kernel && !mixed) return launch_tile32(h, p, Nin, N0, Nout, s);
     return launch_impl<float, false>(h, p, Nin, N0, Nout, nullptr, s);
 }
 

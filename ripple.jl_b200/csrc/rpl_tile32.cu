@@ -103,7 +103,8 @@ __device__ __forceinline__ float2 flux2(float2 m3, float2 m2, float2 m1, float2 
 // One CTA's work: stage update of the TX x TY tile `tile` (row-major over the tiles of the grid) for all
 // bins, with TX*TY*L threads. P is TileArgs seen through the kernel parameter bank (single-model kernel)
 // or a shared-memory copy (ensemble kernel).
-// SRC: 0 no sources, 1 the plain FP32 sources, 2 the learned source with per-cell plain fallback.
+// SRC: 0 no sources, 1 the plain FP32 sources, 2 the learned source with per-cell plain fallback,
+// 3 the per-cell-bin rates of SourceTermSet terms (rpl_terms.cu).
 template <int L, int TX, int TY, bool REFRACT, int SRC>
 __device__ __forceinline__ void tile_body(const TileArgs& p, int tile, float* smem) {
     constexpr int RW = TX + 6, RH = TY + 6;   // staged rectangle (only its cross is loaded)
@@ -215,7 +216,7 @@ __device__ __forceinline__ void tile_body(const TileArgs& p, int tile, float* sm
     Bin32 wb0{}, wb1{};
     bool plain_src = SRC == 1;
     const float* lrow = nullptr;
-    if constexpr (SRC != 0) {
+    if constexpr (SRC == 1 || SRC == 2) {
         const int64_t cidx = (int64_t)jc * Nx + ic;
         wc = load_cell32(p.cell32 + 8 * cidx);
         wb0 = load_bin32(p.bin32 + 8 * mc);
@@ -320,9 +321,11 @@ __device__ __forceinline__ void tile_body(const TileArgs& p, int tile, float* sm
                 const float2 cs = __ldg(p.cs32 + n);
                 G.x += source32(p, wc, wb0, cs.x, cs.y, c.x);
                 G.y += source32(p, wc, wb1, cs.x, cs.y, c.y);
-            } else {  // learned: N * rate, rate = lscale * sinh(network output of bin (m, n))
+            } else if (SRC == 2) {  // learned: N * rate, rate = lscale * sinh(network output of bin (m, n))
                 const float2 y = __ldg(reinterpret_cast<const float2*>(lrow + (int64_t)n * Nk));
                 G = fma2(mul2(c, f2(p.lscale)), make_float2(sinhf(y.x), sinhf(y.y)), G);
+            } else {  // SourceTermSet rates of this stage, state layout
+                G = fma2(*reinterpret_cast<const float2*>(p.lin_rates + slice * n + home), c, G);
             }
         }
         // stage update
@@ -400,11 +403,13 @@ template <int L>
 cudaError_t launch_L(const Handle& h, const StageParams& p, const TileArgs& a, cudaStream_t s) {
     const int tiles = (int)(((h.desc.Nx + 7) / 8) * ((h.desc.Ny + 3) / 4));
     const bool refract = p.transport == RPL_TRANSPORT_REFRACTION;
-    const int src = p.learned ? 2 : ((p.has_wind || p.has_diss) ? 1 : 0);
+    const int src = p.learned ? 2 : ((p.has_wind || p.has_diss) ? 1 : (p.lin_rates ? 3 : 0));
     if (refract) {
+        if (src == 3) return launch_variant<L, true, 3>(a, tiles, s);
         if (src == 2) return launch_variant<L, true, 2>(a, tiles, s);
         return src ? launch_variant<L, true, 1>(a, tiles, s) : launch_variant<L, true, 0>(a, tiles, s);
     }
+    if (src == 3) return launch_variant<L, false, 3>(a, tiles, s);
     if (src == 2) return launch_variant<L, false, 2>(a, tiles, s);
     return src ? launch_variant<L, false, 1>(a, tiles, s) : launch_variant<L, false, 0>(a, tiles, s);
 }
@@ -456,6 +461,7 @@ TileArgs make_tile_args(const Handle& h, const StageParams& p, const void* Nin, 
     a.lrate = p.lrate;
     a.lflag = p.lflag;
     a.lscale = p.lscale;
+    a.lin_rates = static_cast<const float*>(p.lin_rates);
     return a;
 }
 

@@ -8,7 +8,9 @@ from ._lib import ArgumentError, RplError, load as load_library, LIB_PATH
 from .grids import (Bounded, Flat, InfiniteDepth, Periodic, PolarWaveVectorGrid, RectilinearGrid,
                     centers_to_faces, lower_bounded_centers_to_faces)
 from .sources import (BulkWindDrag, Clockwise, Counterclockwise, HollandHurricaneWind, LinearStormTrack,
-                      LocalSaturationDissipation, PrecomputedSources, PressureCorrelationInput)
+                      LocalSaturationDissipation, PrecomputedSources, PressureCorrelationInput,
+                      ExponentialWindInput, WaveAgeWindInput, WhitecappingDissipation, MeanSpectrumWhitecapping,
+                      SourceTermSet)
 from .model import (Clock, ProductField, PseudomomentumVelocities, Simulation, SpatialAveraging, SpectralWaveModel, WENO, WaveActionField,
                     compute_tendencies, interior, run_, set_, time_step, update_coupling)
 from .ensemble import Ensemble

@@ -56,6 +56,11 @@ class RplSources(ctypes.Structure):
     ]
 
 
+class RplSourceTerm(ctypes.Structure):
+    _fields_ = [("kind", _i32), ("reserved", _i32), ("rate", _d), ("rate_field", _dp), ("direction", _d),
+                ("speed", _d), ("speed_field", _dp), ("p", _d * 4), ("gravity", _d)]
+
+
 class RplEnsembleOptions(ctypes.Structure):
     _fields_ = [("abi_version", _i32), ("use_graph", _i32), ("autotune", _i32), ("direct_cells", _i32),
                 ("autotune_cache", ctypes.c_char_p)]
@@ -98,6 +103,7 @@ _SIGNATURES = {
     "rpl_update_coupling": (ctypes.c_int, [ctypes.c_void_p]),
     "rpl_set_sources": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(RplSources)]),
     "rpl_set_wind_field": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp]),
+    "rpl_set_source_terms": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(RplSourceTerm), _i32]),
     "rpl_set_action": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, _i32, _i32]),
     "rpl_get_action": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, _i32, _i32]),
     "rpl_set_action_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, _i32, _i32]),
@@ -138,6 +144,8 @@ _SIGNATURES = {
     "rpl_mlp_forward": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, _i64, ctypes.c_void_p]),
     "rpl_gemm_bf16": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, _i32, _i32, _i32,
                                      ctypes.c_void_p]),
+    "rpl_gemm_bf16_bounded": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, _i32, _i32, _i32,
+                                             ctypes.c_uint32, ctypes.c_void_p]),
     "rpl_learned_sample": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                           ctypes.c_void_p]),
     "rpl_set_learned_source": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,

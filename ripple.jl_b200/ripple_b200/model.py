@@ -15,7 +15,7 @@ from . import _lib
 from ._lib import ArgumentError, check, dptr
 from .grids import InfiniteDepth, PolarWaveVectorGrid, RectilinearGrid
 from .sources import (BulkWindDrag, HollandHurricaneWind, LinearStormTrack, LocalSaturationDissipation,
-                      PrecomputedSources, PressureCorrelationInput, evaluate_wind)
+                      PrecomputedSources, PressureCorrelationInput, evaluate_wind, linear_terms, term_record)
 
 
 class WENO:
@@ -445,6 +445,25 @@ class SpectralWaveModel:
 
     # ------------------------------------------------------------------ sources
     def _set_sources(self, sources):
+        terms = linear_terms(sources)
+        if terms is not None:
+            # SourceTermSet (or one such term): rates evaluated on the device before every stage
+            arr = (_lib.RplSourceTerm * max(1, len(terms)))()
+            self._terms_keep = []
+            for k, t in enumerate(terms):
+                kind, rate, rf, direction, speed, sf, prm, grav = term_record(t, self.grid)
+                arr[k].kind, arr[k].rate, arr[k].direction = kind, rate, direction
+                arr[k].speed, arr[k].gravity = speed, grav
+                for q in range(4):
+                    arr[k].p[q] = prm[q]
+                if rf is not None:
+                    self._terms_keep.append(rf)
+                    arr[k].rate_field = dptr(rf)
+                if sf is not None:
+                    self._terms_keep.append(sf)
+                    arr[k].speed_field = dptr(sf)
+            check(self._lib.rpl_set_source_terms(self._h, arr, len(terms)))
+            return
         wind_input, dissipation, cap = None, None, 0
         if isinstance(sources, PrecomputedSources):
             wind_input, dissipation = sources.wind_input, sources.dissipation

@@ -5,7 +5,10 @@ PressureCorrelationInput (src/Physics/WindInput/pressure_correlation.jl:24-52),
 LocalSaturationDissipation (src/Physics/Dissipation/local_saturation.jl:18-28),
 BulkWindDrag (src/Physics/shared/drag.jl:73-86),
 PrecomputedSources (src/Physics/Packages/precomputed_sources.jl:179-191),
-HollandHurricaneWind / LinearStormTrack (src/Forcing/winds.jl:115-229).
+HollandHurricaneWind / LinearStormTrack (src/Forcing/winds.jl:115-229), and the SourceTermSet terms
+whose tendency is linear in the action: ExponentialWindInput, WaveAgeWindInput, WhitecappingDissipation
+(src/Sources/Sources.jl:5-11,32-39,67-122) and MeanSpectrumWhitecapping
+(src/Physics/Dissipation/mean_spectrum.jl:20-40).
 The rates themselves are evaluated by librpl.so on the device.
 """
 import math
@@ -141,3 +144,160 @@ def evaluate_wind(wind, x, y, t):
     vel = wind(X, Y, t)
     vx, vy = (np.asarray(v, dtype=np.float64) for v in vel)
     return np.hypot(vx, vy), np.arctan2(vy, vx)
+
+
+def source_parameter(value, name):
+    """A rate or speed parameter (Sources.jl:480-482): a number, an (Nx, Ny) array, or a callable of
+    (x, y) evaluated once at the cell centres. Time-dependent callables are outside this path."""
+    if value is None:
+        return None
+    if np.isscalar(value):
+        return float(value)
+    if callable(value):
+        return value
+    a = np.asarray(value, dtype=np.float64)
+    if a.ndim != 2:
+        raise ArgumentError(f"{name} must be a number, an (Nx, Ny) array or a callable of (x, y)")
+    return a
+
+
+def _integer_spreading_power(p):
+    """Sources.jl:1387-1392"""
+    if not p >= 0:
+        raise ArgumentError("directional spreading power must be nonnegative")
+    if float(p) != int(p):
+        raise ArgumentError("finite-volume directional spreading currently supports nonnegative integer powers; "
+                            f"got {float(p)}")
+    return int(p)
+
+
+class ExponentialWindInput:
+    """rate * cell average of max(cos(phi - direction), 0)^spreading_power (Sources.jl:32-39,492-496)."""
+
+    def __init__(self, *, rate=0.0, direction=0.0, spreading_power=2.0):
+        self.rate = source_parameter(rate, "rate")
+        if not np.isscalar(direction):
+            raise ArgumentError("ExponentialWindInput direction must be a number on this path")
+        self.direction = float(direction)
+        self.spreading_power = float(spreading_power)
+        _integer_spreading_power(self.spreading_power)
+
+
+class WaveAgeWindInput:
+    """rate * max(U cos / c - threshold, 0)^power * cos^spreading_power (Sources.jl:67-95,522-554)."""
+
+    def __init__(self, *, rate=0.0, speed=None, wind=None, direction=None, inverse_wave_age_threshold=0.83,
+                 power=1.0, spreading_power=1.0, gravity=9.81):
+        speed_value = (10.0 if speed is None else speed) if wind is None else wind
+        direction_value = direction if direction is not None else (0.0 if wind is None else wind)
+        self.rate = source_parameter(rate, "rate")
+        self.speed = source_parameter(speed_value, "speed")
+        if not np.isscalar(direction_value):
+            raise ArgumentError("WaveAgeWindInput direction must be a number on this path")
+        self.direction = float(direction_value)
+        self.inverse_wave_age_threshold = float(inverse_wave_age_threshold)
+        self.power, self.spreading_power, self.gravity = float(power), float(spreading_power), float(gravity)
+        if not self.inverse_wave_age_threshold >= 0:
+            raise ArgumentError("wave-age wind-input threshold must be nonnegative")
+        if not self.power >= 0:
+            raise ArgumentError("wave-age wind-input power must be nonnegative")
+        if not self.spreading_power >= 0:
+            raise ArgumentError("wave-age wind-input spreading power must be nonnegative")
+        if not self.gravity > 0:
+            raise ArgumentError("wave-age wind-input gravity must be positive")
+
+
+class WhitecappingDissipation:
+    """rate * max(m0 / threshold - 1, 0)^saturation_power * <kappa^p> / k_ref^p (Sources.jl:105-122,583-598)."""
+
+    def __init__(self, *, rate=0.0, saturation_threshold=1.0, saturation_power=1.0, wavenumber_power=1.0,
+                 reference_wavenumber=1.0):
+        self.rate = source_parameter(rate, "rate")
+        self.saturation_threshold = float(saturation_threshold)
+        self.saturation_power = float(saturation_power)
+        self.wavenumber_power = float(wavenumber_power)
+        self.reference_wavenumber = float(reference_wavenumber)
+        if not self.saturation_threshold > 0:
+            raise ArgumentError("whitecapping saturation threshold must be positive")
+        if not self.reference_wavenumber > 0:
+            raise ArgumentError("whitecapping reference wavenumber must be positive")
+        if not self.wavenumber_power >= 0:
+            raise ArgumentError("wavenumber power must be nonnegative")
+
+
+class MeanSpectrumWhitecapping:
+    """-C_ds (m0 kbar^2)^2 sigmabar (delta1 k/kbar + delta2 (k/kbar)^2) damping with p-th mean wavenumber and
+    frequency (mean_spectrum.jl:20-40,90-111); BJA defaults."""
+
+    def __init__(self, *, C_ds=-2.1, δ1=0.4, δ2=0.6, p=0.5, gravity=9.81, delta1=None, delta2=None):
+        self.C_ds = float(C_ds)
+        self.δ1 = float(δ1 if delta1 is None else delta1)
+        self.δ2 = float(δ2 if delta2 is None else delta2)
+        self.p, self.gravity = float(p), float(gravity)
+        if self.p == 0:
+            raise ArgumentError("MeanSpectrumWhitecapping needs a nonzero mean exponent p")
+
+
+LINEAR_TERMS = (ExponentialWindInput, WaveAgeWindInput, WhitecappingDissipation, MeanSpectrumWhitecapping)
+
+
+class SourceTermSet:
+    """A sum of source terms (Sources.jl:5-11,443-449): here terms whose tendency is linear in the action."""
+
+    def __init__(self, *terms):
+        if len(terms) == 1 and isinstance(terms[0], (tuple, list)):
+            terms = tuple(terms[0])
+        for t in terms:
+            if not isinstance(t, LINEAR_TERMS):
+                raise ArgumentError(f"source term {type(t).__name__} is outside the B200 path")
+        self.terms = tuple(terms)
+
+    def __len__(self):
+        return len(self.terms)
+
+    def __iter__(self):
+        return iter(self.terms)
+
+
+def linear_terms(sources):
+    """The SourceTermSet terms of a sources argument (a set or one term), or None."""
+    if isinstance(sources, SourceTermSet):
+        return sources.terms
+    if isinstance(sources, LINEAR_TERMS):
+        return (sources,)
+    return None
+
+
+def parameter_field(value, grid):
+    """A source parameter as (scalar, (Nx, Ny) x-fastest field or None) on the grid's cell centres."""
+    if value is None:
+        return 0.0, None
+    if np.isscalar(value):
+        return float(value), None
+    if callable(value):
+        X, Y = np.meshgrid(grid.xnodes(), grid.ynodes(), indexing="ij")
+        value = np.broadcast_to(np.asarray(value(X, Y), dtype=np.float64), (grid.Nx, grid.Ny))
+    a = np.asarray(value, dtype=np.float64)
+    if a.shape != (grid.Nx, grid.Ny):
+        raise ArgumentError(f"source parameter field must have shape {(grid.Nx, grid.Ny)}")
+    return 0.0, np.asfortranarray(a).ravel(order="F").copy()
+
+
+TERM_KIND = {ExponentialWindInput: 1, WaveAgeWindInput: 2, WhitecappingDissipation: 3, MeanSpectrumWhitecapping: 4}
+
+
+def term_record(t, grid):
+    """(kind, rate, rate_field, direction, speed, speed_field, p[4], gravity) of one term."""
+    if isinstance(t, ExponentialWindInput):
+        rate, rf = parameter_field(t.rate, grid)
+        return 1, rate, rf, t.direction, 0.0, None, (t.spreading_power, 0.0, 0.0, 0.0), 9.81
+    if isinstance(t, WaveAgeWindInput):
+        rate, rf = parameter_field(t.rate, grid)
+        speed, sf = parameter_field(t.speed, grid)
+        return 2, rate, rf, t.direction, speed, sf, (t.inverse_wave_age_threshold, t.power, t.spreading_power,
+                                                    0.0), t.gravity
+    if isinstance(t, WhitecappingDissipation):
+        rate, rf = parameter_field(t.rate, grid)
+        return 3, rate, rf, 0.0, 0.0, None, (t.saturation_threshold, t.saturation_power, t.wavenumber_power,
+                                            t.reference_wavenumber), 9.81
+    return 4, 0.0, None, 0.0, 0.0, None, (t.C_ds, t.δ1, t.δ2, t.p), t.gravity

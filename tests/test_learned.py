@@ -44,6 +44,28 @@ def test_gemm_rejects_bad_shapes(torch):
     assert lib.rpl_gemm_bf16(learned._ptr(A), learned._ptr(A), learned._ptr(C), 100, 128, 64, None) != 0
 
 
+def test_gemm_bounded_wait_runs_out_and_recovers(torch):
+    """A poll limit of one makes the first barrier wait give up (a TMA load takes far longer than one
+    poll): the kernel drains its loads and MMAs, frees its tensor memory and returns; the call reports
+    RPL_ERR_DEVICE with error bit 4, and the next GEMM with the default limit on the same context is
+    correct."""
+    M, N, K = 1024, 512, 1152
+    g = torch.Generator(device="cuda").manual_seed(3)
+    A = torch.randn(M, K, device="cuda", generator=g).to(torch.bfloat16)
+    B = torch.randn(N, K, device="cuda", generator=g).to(torch.bfloat16)
+    C = torch.zeros(M, N, device="cuda", dtype=torch.float32)
+    torch.cuda.synchronize()
+    lib = rp.load_library()
+    st = lib.rpl_gemm_bf16_bounded(learned._ptr(A), learned._ptr(B), learned._ptr(C), M, N, K, 1, None)
+    assert st == rp._lib.RPL_ERR_DEVICE
+    assert b"bounded wait ran out" in lib.rpl_last_error()
+    torch.cuda.synchronize()                                  # no sticky CUDA error
+    rp._lib.check(lib.rpl_gemm_bf16_bounded(learned._ptr(A), learned._ptr(B), learned._ptr(C), M, N, K, 0, None))
+    ref = A.double() @ B.double().T
+    scale = (A.double().norm(dim=1)[:, None] * B.double().norm(dim=1)[None, :])
+    assert float(((C.double() - ref).abs() / scale).max()) <= 1e-5
+
+
 def small_net_and_batch(torch, nbins=256, hidden=256, B=256, seed=1):
     net = learned.SourceNetwork(nbins=nbins, hidden=hidden, rows=256, seed=seed)
     g = torch.Generator(device="cuda").manual_seed(seed)
