@@ -221,6 +221,16 @@ int rpl_step_async(rpl_handle* h, double dt, int64_t nsteps);
 /* Launches exactly one RK3 stage (1, 2 or 3) of the step starting at the current clock; for
  * per-kernel timing. Stage 3 advances the clock. */
 int rpl_stage_async(rpl_handle* h, double dt, int32_t stage);
+/* Part of one RK3 stage for a decomposed domain (no counterpart in the reference): the stage kernel
+ * updates rows row0 .. row0+nrows-1 only (nrows may be 0); RPL_STAGE_PREPARE first runs the stage's
+ * column-local preparation kernels (wind, stress cap, pseudomomentum refresh, source-term rates) over
+ * every row, RPL_STAGE_FINISH completes the stage (after stage 3: SpatialAveraging, clock advance).
+ * A stage split into launches gives exactly the full stage when the row ranges cover the rows once, the
+ * first launch prepares and the last finishes. rpl_stage_async(h, dt, s) is
+ * rpl_stage_rows_async(h, dt, s, 0, Ny, RPL_STAGE_PREPARE | RPL_STAGE_FINISH). */
+#define RPL_STAGE_PREPARE 1
+#define RPL_STAGE_FINISH 2
+int rpl_stage_rows_async(rpl_handle* h, double dt, int32_t stage, int64_t row0, int64_t nrows, int32_t flags);
 int rpl_sync(rpl_handle* h);
 /* Use the caller's CUDA stream (a cudaStream_t on the handle's device) instead of the handle's own. */
 int rpl_set_stream(rpl_handle* h, void* stream);
@@ -249,6 +259,10 @@ int rpl_diagnostics_device(rpl_handle* h, double* m0, double* hs, double* krms, 
  * boundary rows out, exchanges them, copies them into the halo rows, then runs rpl_stage_async. */
 int rpl_rows_get(rpl_handle* h, int32_t which, int64_t row0, int64_t nrows, void* dst);
 int rpl_rows_set(rpl_handle* h, int32_t which, int64_t row0, int64_t nrows, const void* src);
+/* The same copies on the caller's stream (a cudaStream_t on the handle's device), so that an exchange
+ * can run beside the stage kernel of the rows that do not read the halo (rpl_stage_rows_async). */
+int rpl_rows_get_on(rpl_handle* h, int32_t which, int64_t row0, int64_t nrows, void* dst, void* stream);
+int rpl_rows_set_on(rpl_handle* h, int32_t which, int64_t row0, int64_t nrows, const void* src, void* stream);
 
 /* Replaces fetch_output(field::ProductField, model) = interior(field) (OceananigansIntegration.jl:7-9)
  * for output writers: enqueues a copy of the current action, converted to `dtype` in RPL_LAYOUT_XFAST,

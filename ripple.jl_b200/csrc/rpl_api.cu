@@ -139,14 +139,16 @@ int check_error_word(Handle* h) {
     return RPL_OK;
 }
 
-int launch_step(Handle* h, double dt, int stage_only) {
+// One RK3 stage over rows [j_lo, j_hi): the stage's preparation kernels (wind, stress cap or learned
+// rows, pseudomomentum refresh, SourceTermSet rates; all column-local) when `prepare`, the stage kernel,
+// and when `finish` what completes the stage (after stage 3: SpatialAveraging and the clock).
+int launch_stage_rows(Handle* h, double dt, int stage, int64_t j_lo, int64_t j_hi, bool prepare, bool finish) {
     cudaStream_t s = h->stream;
     const bool sources = h->has_sources && (h->src.wind_kind != RPL_WIND_NONE);
-    const int first = stage_only ? stage_only : 1, last = stage_only ? stage_only : 3;
-    for (int stage = first; stage <= last; ++stage) {
-        const void* Nin = stage == 1 ? h->N : (stage == 2 ? h->A : h->B);
-        // with SpatialAveraging, stage 3 writes into A (free by then) and the averaging writes A -> N
-        void* Nout = stage == 1 ? h->A : (stage == 2 ? h->B : (h->smooth ? h->A : h->N));
+    const void* Nin = stage == 1 ? h->N : (stage == 2 ? h->A : h->B);
+    // with SpatialAveraging, stage 3 writes into A (free by then) and the averaging writes A -> N
+    void* Nout = stage == 1 ? h->A : (stage == 2 ? h->B : (h->smooth ? h->A : h->N));
+    if (prepare) {
         if (sources) {
             if (stage == 1) RPL_CUDA(rpl::launch_wind(*h, h->time, s));
             if (h->learned) RPL_CUDA(rpl::launch_learned_stage_prep(*h, Nin, s));
@@ -154,13 +156,26 @@ int launch_step(Handle* h, double dt, int stage_only) {
         }
         if (h->pm) RPL_CUDA(rpl::launch_pm_refresh(*h, Nin, s, false));
         if (h->n_terms) RPL_CUDA(rpl::launch_terms(*h, Nin, s));
-        const rpl::StageParams p = rpl::make_params(*h, dt, stage);
-        RPL_CUDA(rpl::launch_stage(*h, p, Nin, h->N, Nout, s));
-        if (stage == 3 && h->smooth) RPL_CUDA(rpl::launch_smooth(*h, h->A, h->N, dt, s));  // time_step.jl:168
     }
-    if (last == 3) {
+    if (j_hi > j_lo) {
+        rpl::StageParams p = rpl::make_params(*h, dt, stage);
+        p.j_lo = j_lo;
+        p.j_hi = j_hi;
+        RPL_CUDA(rpl::launch_stage(*h, p, Nin, h->N, Nout, s));
+    }
+    if (finish && stage == 3) {
+        if (h->smooth) RPL_CUDA(rpl::launch_smooth(*h, h->A, h->N, dt, s));  // time_step.jl:168
         h->time += dt;
         h->iteration += 1;
+    }
+    return RPL_OK;
+}
+
+int launch_step(Handle* h, double dt, int stage_only) {
+    const int first = stage_only ? stage_only : 1, last = stage_only ? stage_only : 3;
+    for (int stage = first; stage <= last; ++stage) {
+        const int st = launch_stage_rows(h, dt, stage, 0, h->desc.Ny, true, true);
+        if (st) return st;
     }
     return RPL_OK;
 }
@@ -785,6 +800,18 @@ int rpl_stage_async(rpl_handle* hh, double dt, int32_t stage) {
     if ((st = check_step_args(h, dt))) return st;
     if (stage < 1 || stage > 3) return fail(RPL_ERR_ARGUMENT, "stage must be 1, 2 or 3");
     return launch_step(h, dt, stage);
+}
+
+int rpl_stage_rows_async(rpl_handle* hh, double dt, int32_t stage, int64_t row0, int64_t nrows, int32_t flags) {
+    int st = check_handle(hh);
+    if (st) return st;
+    Handle* h = reinterpret_cast<Handle*>(hh);
+    if ((st = check_step_args(h, dt))) return st;
+    if (stage < 1 || stage > 3) return fail(RPL_ERR_ARGUMENT, "stage must be 1, 2 or 3");
+    if (row0 < 0 || nrows < 0 || row0 + nrows > h->desc.Ny) return fail(RPL_ERR_ARGUMENT, "rows out of range");
+    if (flags & ~(RPL_STAGE_PREPARE | RPL_STAGE_FINISH)) return fail(RPL_ERR_ARGUMENT, "unknown stage flags");
+    return launch_stage_rows(h, dt, stage, row0, row0 + nrows, (flags & RPL_STAGE_PREPARE) != 0,
+                             (flags & RPL_STAGE_FINISH) != 0);
 }
 
 int rpl_sync(rpl_handle* hh) {

@@ -21,7 +21,8 @@ int hfail(int code, const std::string& msg) {
     return code;
 }
 
-int rows_copy(rpl_handle* hh, int32_t which, int64_t row0, int64_t nrows, void* packed, bool out) {
+int rows_copy(rpl_handle* hh, int32_t which, int64_t row0, int64_t nrows, void* packed, bool out,
+              cudaStream_t stream, bool own_stream) {
     if (!hh) return hfail(RPL_ERR_ARGUMENT, "null handle");
     Handle* h = reinterpret_cast<Handle*>(hh);
     cudaError_t e = cudaSetDevice(h->device);
@@ -34,8 +35,9 @@ int rows_copy(rpl_handle* hh, int32_t which, int64_t row0, int64_t nrows, void* 
     const size_t row_bytes = (size_t)(d.Nx * d.Nk) * h->elem;
     const size_t width = (size_t)nrows * row_bytes, pitch = (size_t)d.Ny * row_bytes;
     char* rows = state + (size_t)row0 * row_bytes;
-    e = out ? cudaMemcpy2DAsync(packed, width, rows, pitch, width, (size_t)d.Np, cudaMemcpyDeviceToDevice, h->stream)
-            : cudaMemcpy2DAsync(rows, pitch, packed, width, width, (size_t)d.Np, cudaMemcpyDeviceToDevice, h->stream);
+    if (own_stream) stream = h->stream;
+    e = out ? cudaMemcpy2DAsync(packed, width, rows, pitch, width, (size_t)d.Np, cudaMemcpyDeviceToDevice, stream)
+            : cudaMemcpy2DAsync(rows, pitch, packed, width, width, (size_t)d.Np, cudaMemcpyDeviceToDevice, stream);
     if (e != cudaSuccess) {
         cudaGetLastError();
         return hfail(RPL_ERR_CUDA, std::string(out ? "rpl_rows_get: " : "rpl_rows_set: ") + cudaGetErrorString(e));
@@ -48,11 +50,19 @@ int rows_copy(rpl_handle* hh, int32_t which, int64_t row0, int64_t nrows, void* 
 extern "C" {
 
 int rpl_rows_get(rpl_handle* h, int32_t which, int64_t row0, int64_t nrows, void* dst) {
-    return rows_copy(h, which, row0, nrows, dst, true);
+    return rows_copy(h, which, row0, nrows, dst, true, nullptr, true);
 }
 
 int rpl_rows_set(rpl_handle* h, int32_t which, int64_t row0, int64_t nrows, const void* src) {
-    return rows_copy(h, which, row0, nrows, const_cast<void*>(src), false);
+    return rows_copy(h, which, row0, nrows, const_cast<void*>(src), false, nullptr, true);
+}
+
+int rpl_rows_get_on(rpl_handle* h, int32_t which, int64_t row0, int64_t nrows, void* dst, void* stream) {
+    return rows_copy(h, which, row0, nrows, dst, true, (cudaStream_t)stream, false);
+}
+
+int rpl_rows_set_on(rpl_handle* h, int32_t which, int64_t row0, int64_t nrows, const void* src, void* stream) {
+    return rows_copy(h, which, row0, nrows, const_cast<void*>(src), false, (cudaStream_t)stream, false);
 }
 
 }  // extern "C"

@@ -57,6 +57,7 @@ struct StageParams {
     float wind_K32, von_karman32, z_alpha32;  // FP32 copies: rho_ratio beta_max / kappa_vk^2, kappa_vk, z_alpha
     unsigned int* err;                      // device error word
     const void* lin_rates;                  // SourceTermSet rates per cell-bin (state layout and type) or null
+    int64_t j_lo, j_hi;                     // rows the stage updates (all: 0, Ny); other rows are not written
 };
 
 // Arguments of one FP32 tile-kernel stage launch over one model (rpl_tile32.cu): the buffers and the
@@ -81,6 +82,7 @@ struct TileArgs {
     const unsigned int* lflag;
     int learned, pad1;
     const float* lin_rates;  // SourceTermSet rates per cell-bin (state layout) or null
+    int j_lo, j_hi;          // rows the stage updates
 };
 
 // Tile shapes (kappa-pair lanes per cell L, tile TX x TY) compiled into the ensemble kernel; every

@@ -192,10 +192,10 @@ __global__ void __launch_bounds__(BLOCK) column_kernel(const T* __restrict__ Nin
     const int m = lane & (SEG - 1);
     const int base = lane - m;
     const int Nx = (int)p.Nx, Ny = (int)p.Ny, Nk = (int)p.Nk, Np = (int)p.Np;
-    const int64_t P = (int64_t)Nx * Ny;
+    const int64_t P = (int64_t)Nx * Ny, Pr = (int64_t)Nx * (p.j_hi - p.j_lo);  // Pr: cells of the updated rows
     const int64_t col = ((int64_t)blockIdx.x * (BLOCK / 32) + warp) * CPW + lane / SEG;
-    const bool live = col < P && m < Nk;
-    const int64_t cc = col < P ? col : P - 1;
+    const bool live = col < Pr && m < Nk;
+    const int64_t cc = (col < Pr ? col : Pr - 1) + (int64_t)Nx * p.j_lo;
     const int mm = m < Nk ? m : Nk - 1;
     const int i = (int)(cc % Nx), j = (int)(cc / Nx);
     const Coef q = load_coef(p.coef + 8 * (cc * Nk + mm));
@@ -309,6 +309,7 @@ __global__ void __launch_bounds__(BLOCK) generic_kernel(const T* __restrict__ Ni
     const int64_t c = cn % P;
     const int n = (int)(cn / P);
     const int i = (int)(c % Nx), j = (int)(c / Nx);
+    if (j < p.j_lo || j >= p.j_hi) return;
     const Coef q = load_coef(p.coef + 8 * (c * Nk + m));
     const double cph = p.cosp[n], sph = p.sinp[n];
     T ux, uy, ck, cp;
@@ -360,6 +361,8 @@ __global__ void __launch_bounds__(BLOCK) source_only_kernel(const T* __restrict_
     if (t >= slice * p.Np) return;
     const int m = (int)(t % p.Nk);
     const int64_t cn = t / p.Nk;
+    const int64_t jr = (cn % P) / p.Nx;
+    if (jr < p.j_lo || jr >= p.j_hi) return;
     const T a = Nin[t];
     T G = T(0);
     if (p.has_wind || p.has_diss) G = T(source_term(p, cn % P, m, (int)(cn / P), (double)a));
@@ -376,7 +379,7 @@ __global__ void __launch_bounds__(BLOCK) source_only_kernel(const T* __restrict_
 template <typename T, bool TEND>
 cudaError_t launch_impl(const Handle& h, const StageParams& p, const void* Nin, const void* N0, void* Nout, double* G,
                         cudaStream_t s) {
-    const int64_t P = h.desc.Nx * h.desc.Ny, Nk = h.desc.Nk;
+    const int64_t Nk = h.desc.Nk;
     const bool refract = p.transport == RPL_TRANSPORT_REFRACTION;
     const T* in = (const T*)Nin;
     const T* n0 = (const T*)N0;
@@ -387,7 +390,8 @@ cudaError_t launch_impl(const Handle& h, const StageParams& p, const void* Nin, 
     } else if (Nk <= 32) {
         const int seg = Nk <= 4 ? 4 : Nk <= 8 ? 8 : Nk <= 16 ? 16 : 32;
         const int64_t cols_per_block = (BLOCK / 32) * (32 / seg);
-        const dim3 grid((unsigned)((P + cols_per_block - 1) / cols_per_block));
+        const int64_t Pr = h.desc.Nx * (p.j_hi - p.j_lo);
+        const dim3 grid((unsigned)((Pr + cols_per_block - 1) / cols_per_block));
 #define RPL_COL(SEGV)                                                                                        \
     if (seg == SEGV) {                                                                                       \
         if (refract) column_kernel<T, SEGV, true, TEND><<<grid, BLOCK, 0, s>>>(in, n0, out, G, p);          \
@@ -451,6 +455,8 @@ StageParams make_params(const Handle& h, double dt, int stage) {
     p.z_alpha32 = (float)p.z_alpha;
     p.err = h.d_err;
     p.lin_rates = h.n_terms ? h.d_lin_rates : nullptr;
+    p.j_lo = 0;
+    p.j_hi = d.Ny;
     return p;
 }
 

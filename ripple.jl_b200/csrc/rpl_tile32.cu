@@ -117,14 +117,14 @@ __device__ __forceinline__ void tile_body(const TileArgs& p, int tile, float* sm
     const int Nx = p.Nx, Ny = p.Ny, Nk = p.Nk, Np = p.Np;
     const int64_t slice = (int64_t)Nx * Ny * Nk;
     const int tiles_x = (Nx + TX - 1) / TX;
-    const int i0 = (tile % tiles_x) * TX, j0 = (tile / tiles_x) * TY;
+    const int i0 = (tile % tiles_x) * TX, j0 = p.j_lo + (tile / tiles_x) * TY;  // tiles over rows [j_lo, j_hi)
     const int tid = threadIdx.x;
     const int l = tid % L;                    // lane within the cell
     const int cell = tid / L;                 // 0 .. TX*TY-1
     const int cx = cell % TX, cy = cell / TX;
     const int i = i0 + cx, j = j0 + cy;
-    const bool live_cell = i < Nx && j < Ny;
-    const int ic = i < Nx ? i : Nx - 1, jc = j < Ny ? j : Ny - 1;
+    const bool live_cell = i < Nx && j < p.j_hi;
+    const int ic = i < Nx ? i : Nx - 1, jc = j < p.j_hi ? j : p.j_hi - 1;
     const int m0 = 2 * l;                      // this lane's kappa pair (m0, m0+1)
     const bool live = live_cell && m0 < Nk;
     const int mc = m0 < Nk ? m0 : Nk - 2;
@@ -401,7 +401,7 @@ cudaError_t launch_variant(const TileArgs& a, int tiles, cudaStream_t s) {
 
 template <int L>
 cudaError_t launch_L(const Handle& h, const StageParams& p, const TileArgs& a, cudaStream_t s) {
-    const int tiles = (int)(((h.desc.Nx + 7) / 8) * ((h.desc.Ny + 3) / 4));
+    const int tiles = (int)(((h.desc.Nx + 7) / 8) * ((p.j_hi - p.j_lo + 3) / 4));
     const bool refract = p.transport == RPL_TRANSPORT_REFRACTION;
     const int src = p.learned ? 2 : ((p.has_wind || p.has_diss) ? 1 : (p.lin_rates ? 3 : 0));
     if (refract) {
@@ -462,6 +462,8 @@ TileArgs make_tile_args(const Handle& h, const StageParams& p, const void* Nin, 
     a.lflag = p.lflag;
     a.lscale = p.lscale;
     a.lin_rates = static_cast<const float*>(p.lin_rates);
+    a.j_lo = (int)p.j_lo;
+    a.j_hi = (int)p.j_hi;
     return a;
 }
 

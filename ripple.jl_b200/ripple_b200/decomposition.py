@@ -15,12 +15,21 @@ The exchange per stage: rows are copied out of the stage's input buffer into pac
 GPUs; gloo between CPU processes in the tests), and copied into the halo rows (rpl_rows_set).
 Pseudomomentum coupling and SpatialAveraging are not decomposed (the averaging would need a halo
 exchange between stage 3 and the averaging).
+
+Overlap (rk3_steps_overlapped): an owned row r reads rows r-3 .. r+3, so the owned rows at least 3
+rows from either slab edge (local rows [6, ny)) read no halo row. Each stage first launches those
+rows, then exchanges the stage input's halos on a stream of its own beside that launch, then launches
+the 3 + 3 boundary rows once the halos have arrived. Halo rows are not updated (their values come from
+the neighbours before every use).
 """
+import copy
+
 import numpy as np
 
 from ._lib import ArgumentError, check
 from . import _lib
 from .grids import RectilinearGrid
+from .sources import SourceTermSet, linear_terms
 from .workloads import Workload
 
 HALO = 3
@@ -106,26 +115,89 @@ def local_workload(w, slab):
                for k, v in w.velocities.items()}
         if "q_grid" in vel:
             raise ArgumentError("give the currents on the wave grid's own vertical grid")
+    sources = w.sources
+    terms = linear_terms(sources)
+    if terms is not None:
+        # (Nx, Ny) rate and speed arrays of SourceTermSet terms: the slab's rows (callables of (x, y) are
+        # evaluated on the slab grid, whose owned rows have the parent's nodes)
+        local = []
+        for t in terms:
+            t = copy.copy(t)
+            for name in ("rate", "speed"):
+                v = getattr(t, name, None)
+                if isinstance(v, np.ndarray):
+                    setattr(t, name, np.take(v, rows, axis=1))
+            local.append(t)
+        sources = SourceTermSet(*local)
     return Workload(f"{w.name}[rows {slab.start}:{slab.stop}]", grid, w.spectral_grid, depth, N0, w.dt, w.nsteps,
-                    velocities=vel, sources=w.sources, horizontal_advection=w.horizontal_advection,
+                    velocities=vel, sources=sources, horizontal_advection=w.horizontal_advection,
                     notes=dict(w.notes, slab=(slab.start, slab.stop)))
 
 
-class LibBackend:
-    """The slab's model in librpl.so: row copies and single stages on the handle's stream."""
+def interior_rows(slab):
+    """Local rows [first, stop) whose update reads no halo row (may be empty)."""
+    h, ny = slab.halo, slab.ny
+    lo = min(2 * h, h + ny)
+    return lo, max(ny, lo)
 
-    def __init__(self, model):
+
+def boundary_rows(slab):
+    """The two local row ranges [first, stop) of owned rows that read the low and the high halo."""
+    h, ny = slab.halo, slab.ny
+    lo, hi = interior_rows(slab)
+    return (h, lo), (hi, h + ny)
+
+
+class LibBackend:
+    """The slab's model in librpl.so: row copies and (partial) stages on the handle's stream; with an
+    exchange stream, the row copies of an exchange run on it between begin_exchange and end_exchange."""
+
+    def __init__(self, model, compute_stream=None, exchange_stream=None):
         self.model = model
         self.lib, self.h = model._lib, model.handle
+        self.compute, self.xstream = compute_stream, exchange_stream
+        if exchange_stream is not None:
+            import torch
+            self.ev_in = torch.cuda.Event()
+            self.ev_x = torch.cuda.Event()
+
+    def _stream_arg(self):
+        return _lib.ctypes.c_void_p(self.xstream.cuda_stream)
 
     def rows_get(self, which, first, count, buf):
-        check(self.lib.rpl_rows_get(self.h, which, first, count, _lib.ctypes.c_void_p(buf.data_ptr())))
+        ptr = _lib.ctypes.c_void_p(buf.data_ptr())
+        if self.xstream is not None:
+            check(self.lib.rpl_rows_get_on(self.h, which, first, count, ptr, self._stream_arg()))
+        else:
+            check(self.lib.rpl_rows_get(self.h, which, first, count, ptr))
 
     def rows_set(self, which, first, count, buf):
-        check(self.lib.rpl_rows_set(self.h, which, first, count, _lib.ctypes.c_void_p(buf.data_ptr())))
+        ptr = _lib.ctypes.c_void_p(buf.data_ptr())
+        if self.xstream is not None:
+            check(self.lib.rpl_rows_set_on(self.h, which, first, count, ptr, self._stream_arg()))
+        else:
+            check(self.lib.rpl_rows_set(self.h, which, first, count, ptr))
 
     def stage(self, dt, s):
         check(self.lib.rpl_stage_async(self.h, float(dt), int(s)))
+
+    def stage_rows(self, dt, s, first, count, prepare, finish):
+        flags = (_lib.RPL_STAGE_PREPARE if prepare else 0) | (_lib.RPL_STAGE_FINISH if finish else 0)
+        check(self.lib.rpl_stage_rows_async(self.h, float(dt), int(s), int(first), int(count), flags))
+
+    def mark_input(self):
+        """The stage's input is final on the compute stream (before the interior launch)."""
+        if self.xstream is not None:
+            self.ev_in.record(self.compute)
+
+    def begin_exchange(self):
+        if self.xstream is not None:
+            self.xstream.wait_event(self.ev_in)
+
+    def end_exchange(self):
+        if self.xstream is not None:
+            self.ev_x.record(self.xstream)
+            self.compute.wait_event(self.ev_x)
 
     def sync(self):
         check(self.lib.rpl_sync(self.h))
@@ -138,11 +210,16 @@ def _buffers(slab, Nx, Nk, Np, dtype, device):
     return {k: torch.empty(n, dtype=dtype, device=device) for k in ("send_low", "send_high", "recv_low", "recv_high")}
 
 
-def exchange_dist(backend, slab, which, bufs, group=None):
+def exchange_dist(backend, slab, which, bufs, group=None, stream=None):
     """Refresh the halo rows of buffer `which` from the neighbouring ranks: owned high rows go up to the
     next rank's bottom halo, then owned low rows go down to the previous rank's top halo. Each phase is
     one send and one receive per rank, so ranks that are each other's previous and next (two ranks) pair
-    their messages unambiguously."""
+    their messages unambiguously. With `stream` (a torch CUDA stream) the copies and the point-to-point
+    operations are enqueued on it."""
+    if stream is not None:
+        import torch
+        with torch.cuda.stream(stream):
+            return exchange_dist(backend, slab, which, bufs, group)
     import torch.distributed as dist
     backend.rows_get(which, *slab.send_low(), bufs["send_low"])
     backend.rows_get(which, *slab.send_high(), bufs["send_high"])
@@ -173,6 +250,31 @@ def exchange_local(backends, slabs, which, bufs):
         b.rows_set(which, *s.halo_high(), q["recv_high"])
 
 
+def rk3_steps_overlapped(backends, slabs, exchange, dt, nsteps, before_step=None):
+    """nsteps decomposed SSP-RK3 steps with the exchange beside the interior rows: per stage every slab
+    launches its interior rows (with the stage's preparation kernels), the halos of the stage's input
+    are exchanged (exchange(which), between the backends' begin_exchange and end_exchange), then every
+    slab launches its two boundary row ranges (the last one finishes the stage)."""
+    for _ in range(nsteps):
+        if before_step is not None:
+            before_step()
+        for s, which in ((1, 0), (2, 1), (3, 2)):
+            for b, sl in zip(backends, slabs):
+                b.mark_input()
+                lo, hi = interior_rows(sl)
+                b.stage_rows(dt, s, lo, hi - lo, True, False)
+            for b in backends:
+                b.begin_exchange()
+            exchange(which)
+            for b, sl in zip(backends, slabs):
+                b.end_exchange()
+                (l0, l1), (h0, h1) = boundary_rows(sl)
+                b.stage_rows(dt, s, l0, l1 - l0, False, False)
+                b.stage_rows(dt, s, h0, h1 - h0, False, True)
+    for b in backends:
+        b.sync()
+
+
 def rk3_steps(backends, exchange, dt, nsteps, before_step=None):
     """nsteps decomposed SSP-RK3 steps: before stage s the halo rows of its input buffer (N, A, B) are
     exchanged, then every slab runs the stage."""
@@ -191,7 +293,7 @@ class DecomposedModel:
     """This rank's slab of a workload, advanced with halo exchanges over torch.distributed (one process
     per GPU, NCCL). interior() is the owned rows' action; gather() assembles the global field on rank 0."""
 
-    def __init__(self, w, precision="fp64", group=None, device=0):
+    def __init__(self, w, precision="fp64", group=None, device=0, overlap=True):
         import torch
         import torch.distributed as dist
         self.group = group
@@ -199,11 +301,13 @@ class DecomposedModel:
         self.slab = Slab(w.grid.Ny, world, rank)
         self.local = local_workload(w, self.slab)
         self.model = self.local.model(precision, device=device)
-        # one stream for the library's kernels, the row copies and the exchange (a stream of its own: the
-        # legacy default stream does not order against the library's non-blocking streams)
+        # a stream for the library's kernels (of its own: the legacy default stream does not order against
+        # the library's non-blocking streams); with overlap, the exchange runs on a second stream
         self.stream = torch.cuda.Stream(device)
         check(self.model._lib.rpl_set_stream(self.model.handle, _lib.ctypes.c_void_p(self.stream.cuda_stream)))
-        self.backend = LibBackend(self.model)
+        self.overlap = overlap
+        self.xstream = torch.cuda.Stream(device) if overlap else None
+        self.backend = LibBackend(self.model, self.stream, self.xstream)
         Nk, Np = w.spectral_grid.coordinate_size()
         self.bufs = _buffers(self.slab, w.grid.Nx, Nk, Np, torch.float32 if precision == "fp32" else torch.float64,
                              f"cuda:{device}")
@@ -212,10 +316,17 @@ class DecomposedModel:
         import torch
         m = self.model
         check(m._lib.rpl_set_clock(m.handle, m.clock.time, m.clock.iteration))
+        before = m._push_field_wind if m._field_wind is not None else None
         with torch.cuda.stream(self.stream):
-            rk3_steps([self.backend],
-                      lambda which: exchange_dist(self.backend, self.slab, which, self.bufs, self.group),
-                      dt, nsteps, before_step=m._push_field_wind if m._field_wind is not None else None)
+            if self.overlap:
+                rk3_steps_overlapped([self.backend], [self.slab],
+                                     lambda which: exchange_dist(self.backend, self.slab, which, self.bufs,
+                                                                 self.group, self.xstream),
+                                     dt, nsteps, before_step=before)
+            else:
+                rk3_steps([self.backend],
+                          lambda which: exchange_dist(self.backend, self.slab, which, self.bufs, self.group),
+                          dt, nsteps, before_step=before)
         m.clock.last_Δt = dt
         return self
 

@@ -56,13 +56,40 @@ class OracleBackend:
             self.N[...] = relu((1.0 / 3.0) * self.N + (2.0 / 3.0) * st)
             self.t += dt
 
+    def stage_rows(self, dt, s, first, count, prepare, finish):
+        """The stage for rows [first, first + count) only, from the buffers as they are now (halo rows
+        included, refreshed or not), like rpl_stage_rows_async."""
+        if count > 0:
+            r = slice(first, first + count)
+            if s == 1:
+                self.A[:, r] = relu(self.N + dt * self.o.tendency(self.N, self.t))[:, r]
+            elif s == 2:
+                st = relu(self.A + dt * self.o.tendency(self.A, self.t))
+                self.B[:, r] = relu(0.75 * self.N + 0.25 * st)[:, r]
+            else:
+                st = relu(self.B + dt * self.o.tendency(self.B, self.t))
+                self.N[:, r] = relu((1.0 / 3.0) * self.N + (2.0 / 3.0) * st)[:, r]
+        if finish and s == 3:
+            self.t += dt
+
+    def mark_input(self):
+        pass
+
+    def begin_exchange(self):
+        pass
+
+    def end_exchange(self):
+        pass
+
     def sync(self):
         pass
 
 
 def cases():
+    from test_source_terms import random_terms_workload
     return [workloads.seamount_eddies(N=24, Nz=8, Nk=8, Np=12, nsteps=3),   # currents, depth field
-            workloads.hurricane_swell(N=24, Nk=8, Np=12, nsteps=3)]          # sources, moving storm
+            workloads.hurricane_swell(N=24, Nk=8, Np=12, nsteps=3),          # sources, moving storm
+            random_terms_workload(N=12, Nk=8, Np=12)]                        # SourceTermSet, a rate field
 
 
 def _buffers(slab, w):
@@ -125,7 +152,37 @@ def test_oracle_slabs_in_one_process_equal_the_global_run(oracle_mod, case, worl
     assert np.array_equal(got, ref)
 
 
-def _gloo_rank(rank, world, port, case, out):
+@pytest.mark.parametrize("case", [0, 1, 2])
+@pytest.mark.parametrize("world", [1, 2, 3])
+def test_oracle_overlapped_slabs_equal_the_global_run(oracle_mod, case, world):
+    """Interior rows computed before the exchange (their halo rows still hold the previous stage's
+    values), boundary rows after it: a row that read a halo in the interior launch would differ."""
+    w = cases()[case]
+    slabs = [dc.Slab(w.grid.Ny, world, r) for r in range(world)]
+    backs = [OracleBackend(oracle_mod, dc.local_workload(w, s)) for s in slabs]
+    for b in backs:                                   # halos start wrong: only exchanges may fill them
+        for arr in (b.N, b.A, b.B):
+            arr[:, :3] = -7.0
+            arr[:, -3:] = -7.0
+    bufs = [_buffers(s, w) for s in slabs]
+    dc.rk3_steps_overlapped(backs, slabs, lambda which: dc.exchange_local(backs, slabs, which, bufs), w.dt, 3)
+    got = np.concatenate([b.N[:, s.owned()] for b, s in zip(backs, slabs)], axis=1)
+    ref, _ = oracle_mod.Oracle(w).step(w.N0, w.dt, 3)
+    assert np.array_equal(got, ref)
+
+
+def test_interior_and_boundary_rows_cover_the_owned_rows_once():
+    for Ny, world in ((24, 2), (9, 3), (40, 4), (12, 1)):
+        for r in range(world):
+            s = dc.Slab(Ny, world, r)
+            (l0, l1), (h0, h1) = dc.boundary_rows(s)
+            i0, i1 = dc.interior_rows(s)
+            rows = list(range(l0, l1)) + list(range(i0, i1)) + list(range(h0, h1))
+            assert rows == list(range(s.halo, s.halo + s.ny))
+            assert all(r - 3 >= s.halo and r + 3 < s.halo + s.ny for r in range(i0, i1))
+
+
+def _gloo_rank(rank, world, port, case, out, overlap=False):
     import torch.distributed as dist
     os.environ["MASTER_ADDR"], os.environ["MASTER_PORT"] = "127.0.0.1", str(port)
     import datetime
@@ -136,7 +193,11 @@ def _gloo_rank(rank, world, port, case, out):
         slab = dc.Slab(w.grid.Ny, world, rank)
         back = OracleBackend(oracle_mod, dc.local_workload(w, slab))
         bufs = _buffers(slab, w)
-        dc.rk3_steps([back], lambda which: dc.exchange_dist(back, slab, which, bufs), w.dt, 3)
+        if overlap:
+            dc.rk3_steps_overlapped([back], [slab], lambda which: dc.exchange_dist(back, slab, which, bufs),
+                                    w.dt, 3)
+        else:
+            dc.rk3_steps([back], lambda which: dc.exchange_dist(back, slab, which, bufs), w.dt, 3)
         parts = [None] * world
         dist.all_gather_object(parts, (slab.start, back.N[:, slab.owned()]))
         if rank == 0:
@@ -151,11 +212,12 @@ def _free_port():
         return s.getsockname()[1]
 
 
-@pytest.mark.parametrize("world,case", [(2, 0), (3, 0), (2, 1)])
-def test_oracle_slabs_across_gloo_ranks_equal_the_global_run(oracle_mod, tmp_path, world, case):
+@pytest.mark.parametrize("world,case,overlap", [(2, 0, False), (3, 0, False), (2, 1, False), (2, 0, True),
+                                                 (3, 1, True)])
+def test_oracle_slabs_across_gloo_ranks_equal_the_global_run(oracle_mod, tmp_path, world, case, overlap):
     import torch.multiprocessing as mp
     out = str(tmp_path / "global.npy")
-    mp.start_processes(_gloo_rank, args=(world, _free_port(), case, out), nprocs=world, join=True,
+    mp.start_processes(_gloo_rank, args=(world, _free_port(), case, out, overlap), nprocs=world, join=True,
                        start_method="spawn")
     w = cases()[case]
     ref, _ = oracle_mod.Oracle(w).step(w.N0, w.dt, 3)
@@ -186,6 +248,40 @@ def test_library_slabs_on_one_gpu_equal_the_global_model(case, precision, world)
 
     with torch.cuda.stream(st):
         dc.rk3_steps(backs, lambda which: dc.exchange_local(backs, slabs, which, bufs), w.dt, 3)
+    got = np.concatenate([m.action.interior()[:, s.owned()] for m, s in zip(models, slabs)], axis=1)
+    g = w.model(precision)
+    rp.time_step(g, w.dt, 3)
+    assert np.array_equal(got, g.action.interior())
+    assert all(m.clock.iteration == 3 for m in models)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_library_overlapped_slabs_on_one_gpu_equal_the_global_model(precision):
+    """Row-range stage launches (interior rows, then the two boundary ranges) on one compute stream, the
+    exchange copies on a second stream ordered by events, halo rows never recomputed."""
+    import torch
+    w = cases()[0]
+    if precision == "fp32":
+        w.N0 = w.N0.astype(np.float32, order="F")
+    world = 2
+    slabs = [dc.Slab(w.grid.Ny, world, r) for r in range(world)]
+    models = [dc.local_workload(w, s).model(precision) for s in slabs]
+    st, xs = torch.cuda.Stream(), torch.cuda.Stream()
+    for m in models:
+        rp._lib.check(m._lib.rpl_set_stream(m.handle, rp._lib.ctypes.c_void_p(st.cuda_stream)))
+    backs = [dc.LibBackend(m, st, xs) for m in models]
+    Nk, Np = w.spectral_grid.coordinate_size()
+    dt_t = torch.float32 if precision == "fp32" else torch.float64
+    bufs = [{k: torch.zeros(Np * 3 * w.grid.Nx * Nk, dtype=dt_t, device="cuda")
+             for k in ("send_low", "send_high", "recv_low", "recv_high")} for _ in slabs]
+
+    def exchange(which):
+        with torch.cuda.stream(xs):
+            dc.exchange_local(backs, slabs, which, bufs)
+
+    with torch.cuda.stream(st):
+        dc.rk3_steps_overlapped(backs, slabs, exchange, w.dt, 3)
     got = np.concatenate([m.action.interior()[:, s.owned()] for m, s in zip(models, slabs)], axis=1)
     g = w.model(precision)
     rp.time_step(g, w.dt, 3)
