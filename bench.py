@@ -47,11 +47,17 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--workload", default="seamount", choices=["seamount", "hurricane", "ensemble", "learned",
-                                                                       "selfcoupled"])
+                                                                       "selfcoupled", "mlp"])
+    ap.add_argument("--rows", type=int, default=65536,
+                    help="network rows per forward pass (--workload mlp: the learned source's GEMMs alone)")
     ap.add_argument("--train-steps", type=int, default=40000, help="Adam steps (--workload learned)")
     ap.add_argument("--snapshots", type=int, default=40, help="training snapshots per storm run (--workload learned)")
     ap.add_argument("--dagger", type=int, default=0,
                     help="rounds of rows collected along learned-source runs, labelled by the plain sources (--workload learned)")
+    ap.add_argument("--feature-pad", type=float, default=0.25,
+                    help="absolute widening of the per-bin log-action input bounds beyond the training rows, in "
+                         "feature units (x 4 in log N); a cell outside the bounds uses the plain sources "
+                         "(--workload learned)")
     ap.add_argument("--calm-fraction", type=float, default=0.05,
                     help="share of cells without source activity kept as training rows (--workload learned)")
     ap.add_argument("--members", type=int, default=64, help="ensemble members (--workload ensemble)")
@@ -713,7 +719,7 @@ def run_learned(args, rank, world, local_rank):
     torch.cuda.synchronize()
     t_data = time.perf_counter() - t0
     # out-of-distribution bounds and output clamps from the plain-source rows only
-    lo, hi = learned.input_bounds(X, E)
+    lo, hi = learned.input_bounds(X, E, feature_pad=args.feature_pad)
     ylo, yhi = learned.output_bounds(T)
     # 2. training (the library's forward/backward/Adam kernels), then rounds of rows gathered along the
     #    network's own trajectories (labelled by the plain sources) and more training
@@ -806,7 +812,7 @@ def run_learned(args, rank, world, local_rank):
                        "total_action_rel_diff": abs(a["total"] - b["total"]) / b["total"],
                        "fallback_cells_last_stage": a["fallback"], "cells": P,
                        "training_rows": rows, "training_steps": args.train_steps * (2 + args.dagger) // 2,
-                       "dagger_rounds": args.dagger, "training_s": t_train,
+                       "dagger_rounds": args.dagger, "feature_pad": args.feature_pad, "training_s": t_train,
                        "data_generation_s": t_data, "losses": losses,
                        "mlp_forward_ms_per_stage": fwd_ms, "mlp_forward_tflops": flops / fwd_ms / 1e9,
                        "mlp_tensor_frac": flops / fwd_ms / 1e9 / bf16_peak, "bf16_peak_tflops": bf16_peak,
@@ -814,6 +820,49 @@ def run_learned(args, rank, world, local_rank):
             "clocks": a["clocks"], "gpu_launches": None,
         }
         print(json.dumps(line), flush=True)
+    net.close()
+
+
+def run_mlp(args, rank, world, local_rank):
+    """The learned source network's forward pass alone (1152 + 4 -> 3 x 512 GELU -> 1152, BF16 tcgen05
+    GEMMs with FP32 accumulation) on --rows random rows: --warmup untimed passes, then --steps timed
+    passes (CUDA events); FLOP/s against the measured BF16 tensor-core peak."""
+    import torch
+    from ripple_b200 import learned
+
+    torch.cuda.set_device(local_rank)
+    nb, hd, n = 32 * 36, 512, args.rows
+    net = learned.SourceNetwork(nbins=nb, hidden=hd, rows=min(n, 65536), seed=5, device=local_rank)
+    g = torch.Generator(device="cuda").manual_seed(3)
+    X = torch.randn((n, nb), device="cuda", generator=g).to(torch.bfloat16)
+    E = torch.randn((n, 4), device="cuda", generator=g)
+    for _ in range(args.warmup):
+        net.forward(X, E)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(args.steps):
+        net.forward(X, E)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / max(1, args.steps)
+    flops = 2.0 * n * (nb * hd + 2 * hd * hd + hd * nb)
+    try:
+        peak = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["bf16_tflops"])
+        kind = "measured"
+    except Exception:
+        peak, kind = 1590.0, "fallback"
+    if rank == 0:
+        tf = flops / ms / 1e9
+        print(json.dumps({"metric": "MLP forward TFLOP/s (learned source network)", "value": tf, "unit": "TFLOP/s",
+                          "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+                          "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16",
+                          "data": "synthetic (random rows)",
+                          "config": {"workload": "learned-source MLP forward", "rows": n,
+                                     "network": f"{nb}+4 -> 3 x {hd} GELU -> {nb}"},
+                          "roofline": {"bound": "tensor", "achieved": tf, "peak": peak, "unit": "TFLOP/s",
+                                       "frac": tf / peak, "peak_kind": kind, "kernel": "gemm_kernel"},
+                          "gpu_launches": 4 * args.steps}), flush=True)
     net.close()
 
 
@@ -886,6 +935,9 @@ def main():
         return
     if args.workload == "learned":
         run_learned(args, rank, world, local_rank)
+        return
+    if args.workload == "mlp":
+        run_mlp(args, rank, world, local_rank)
         return
     if args.decompose:
         run_decomposed(args, rank, world, local_rank)
