@@ -357,7 +357,9 @@ __global__ void total_kernel(const double* __restrict__ m0, int64_t Nx, int64_t 
                              const double* __restrict__ ysp, double* __restrict__ total) {
     __shared__ double ss[1024], cc[1024];
     double s = 0.0, c = 0.0;
-    for (int64_t t = threadIdx.x; t < P; t += blockDim.x) kadd(s, c, m0[t] * xsp[t % Nx] * ysp[t / Nx]);
+    const int64_t Ny = P / Nx;
+    for (int64_t j = 0; j < Ny; ++j)
+        for (int64_t i = threadIdx.x; i < Nx; i += blockDim.x) kadd(s, c, m0[j * Nx + i] * xsp[i] * ysp[j]);
     ss[threadIdx.x] = s;
     cc[threadIdx.x] = c;
     __syncthreads();
