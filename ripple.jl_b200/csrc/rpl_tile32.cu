@@ -11,7 +11,10 @@
 //    step n is the - face of step n+1; the face between the lane's two kappa bins and the face above
 //    them are reconstructed together, the face below comes from the lane underneath (shuffle);
 //  * reciprocals: rcp.approx of t'^2 per indicator (finite for 4(eps+beta) <= 1.8e19, i.e. |N| up to
-//    ~2e9) and of the weight sum: four MUFU ops per face and element.
+//    ~2e9) and of the weight sum: four MUFU ops per face and element;
+//  * upwinding: where a warp's velocities share a sign the stencils are read in upwind order directly,
+//    per-element selects otherwise; 256-thread CTAs, two per SM (the kernel is latency-bound: while one
+//    CTA waits at its per-plane barrier the other issues).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -87,17 +90,46 @@ __device__ __forceinline__ void weno5_pair2(float2 s0, float2 s1, float2 s2, flo
     hi = weno_face2(d2, d3, d4, d5, D2, D3, D4, A2, A3, A4, s3);
 }
 
-// u * (N(+1/2) - N(-1/2)) for a periodic direction from m3..p3, upwinded per element by sign(u).
-// Branch-free (per-element selects), so the four directions' arithmetic can interleave.
-__device__ __forceinline__ float2 flux2(float2 m3, float2 m2, float2 m1, float2 c, float2 p1, float2 p2, float2 p3,
-                                        float2 u) {
+// u * (N(+1/2) - N(-1/2)) for a periodic direction from m3..p3, upwinded per element by sign(u)
+// (per-element selects of the stencil: the general case).
+__device__ __forceinline__ float2 flux2_sel(float2 m3, float2 m2, float2 m1, float2 c, float2 p1, float2 p2, float2 p3,
+                                            float2 u) {
     const bool px = u.x >= 0.0f, py = u.y >= 0.0f;
     float2 lo, hi;
     weno5_pair2(sel2(px, py, m3, p3), sel2(px, py, m2, p2), sel2(px, py, m1, p1), c, sel2(px, py, p1, m1),
                 sel2(px, py, p2, m2), lo, hi);
-    // oriented upwind->downwind: positive u -> hi is +1/2; negative u -> lo is +1/2
     const float2 diff = sub2(hi, lo);
     return mul2(u, make_float2(px ? diff.x : -diff.x, py ? diff.y : -diff.y));
+}
+
+// The x and y fluxes of the cell (u (N(+1/2) - N(-1/2)) each, before the 1/spacing). When the x velocities
+// of every lane of the warp share one sign and so do the y velocities (the common case: |c_g| exceeds the
+// current almost everywhere), one branch-free body per sign pair reads the stencils in upwind order with
+// no per-element selects and lets the two directions' arithmetic interleave; otherwise the per-element
+// form. Both give the reference's upwinding (wave_current_refraction.jl:104-123) bit for bit.
+template <bool XP, bool YP, class VF>
+__device__ __forceinline__ void flux_xy_u(VF V, int RW, float2 c, float2 ux, float2 uy, float2& fx, float2& fy) {
+    float2 xl, xh, yl, yh;
+    if constexpr (XP) weno5_pair2(V(-3), V(-2), V(-1), c, V(1), V(2), xl, xh);
+    else weno5_pair2(V(3), V(2), V(1), c, V(-1), V(-2), xl, xh);
+    if constexpr (YP) weno5_pair2(V(-3 * RW), V(-2 * RW), V(-RW), c, V(RW), V(2 * RW), yl, yh);
+    else weno5_pair2(V(3 * RW), V(2 * RW), V(RW), c, V(-RW), V(-2 * RW), yl, yh);
+    fx = XP ? mul2(ux, sub2(xh, xl)) : mul2(ux, sub2(xl, xh));
+    fy = YP ? mul2(uy, sub2(yh, yl)) : mul2(uy, sub2(yl, yh));
+}
+
+template <class VF>
+__device__ __forceinline__ void flux_xy(VF V, int RW, float2 c, float2 ux, float2 uy, float2& fx, float2& fy) {
+    const bool xp = __all_sync(FULL, ux.x >= 0.0f && ux.y >= 0.0f), xn = __all_sync(FULL, ux.x < 0.0f && ux.y < 0.0f);
+    const bool yp = __all_sync(FULL, uy.x >= 0.0f && uy.y >= 0.0f), yn = __all_sync(FULL, uy.x < 0.0f && uy.y < 0.0f);
+    if (xp && yp) flux_xy_u<true, true>(V, RW, c, ux, uy, fx, fy);
+    else if (xp && yn) flux_xy_u<true, false>(V, RW, c, ux, uy, fx, fy);
+    else if (xn && yp) flux_xy_u<false, true>(V, RW, c, ux, uy, fx, fy);
+    else if (xn && yn) flux_xy_u<false, false>(V, RW, c, ux, uy, fx, fy);
+    else {
+        fx = flux2_sel(V(-3), V(-2), V(-1), c, V(1), V(2), V(3), ux);
+        fy = flux2_sel(V(-3 * RW), V(-2 * RW), V(-RW), c, V(RW), V(2 * RW), V(3 * RW), uy);
+    }
 }
 
 // One CTA's work: stage update of the TX x TY tile `tile` (row-major over the tiles of the grid) for all
@@ -237,7 +269,7 @@ __device__ __forceinline__ void tile_body(const TileArgs& p, int tile, float* sm
         issue(n + 2);
         const float* pl = smem + (n % NB) * plane_floats + ctr;
         // idle lanes (m0 >= Nk) read the last live pair; their results are never stored
-        auto V = [&](int dcol, int) { return *reinterpret_cast<const float2*>(pl + dcol * KP + mc); };
+        auto V1 = [&](int dcol) { return *reinterpret_cast<const float2*>(pl + dcol * KP + mc); };
         const float2 c = *reinterpret_cast<const float2*>(pl + mc);
         // velocities (same expression order as the FP64 path)
         const float4 tg = __ldg(p.trig32 + n);
@@ -255,21 +287,33 @@ __device__ __forceinline__ void tile_body(const TileArgs& p, int tile, float* sm
                                    add2(add2(mul2(f2(tg.x), Uxx), mul2(f2(tg.y), add2(Uyx, Uxy))), mul2(f2(tg.z), Uyy)));
             const float2 cp = sub2(add2(mul2(f2(tg.y), sub2(Uxx, Uyy)), mul2(f2(tg.z), Uyx)), mul2(f2(tg.x), Uxy));
             // x and y
-            const float2 fx = mul2(flux2(V(-3, m0), V(-2, m0), V(-1, m0), c, V(1, m0), V(2, m0), V(3, m0), ux), f2(dx_inv));
-            const float2 fy = mul2(flux2(V(-3 * RW, m0), V(-2 * RW, m0), V(-RW, m0), c, V(RW, m0), V(2 * RW, m0),
-                                         V(3 * RW, m0), uy), f2(dy_inv));
+            float2 fx, fy;
+            flux_xy(V1, RW, c, ux, uy, fx, fy);
+            fx = mul2(fx, f2(dx_inv));
+            fy = mul2(fy, f2(dy_inv));
             // kappa: stencil values of this lane's column (clamped like the reference)
             const float km3 = pl[kcm3], km2 = pl[kcm2], km1 = pl[kcm1];
             const float kp2 = pl[kcp2], kp3 = pl[kcp3], kp4 = pl[kcp4];
             const float k0 = c.x, k1 = c.y;
             // face a (m0|m0+1) upwinded by cell m0, face b (m0+1|m0+2) by cell m0+1
             const bool pa = ck.x >= 0.f, pb = ck.y >= 0.f;
-            const float2 sa0 = make_float2(pa ? km2 : kp3, pb ? km1 : kp4);
-            const float2 sa1 = make_float2(pa ? km1 : kp2, pb ? k0 : kp3);
-            const float2 sa2 = make_float2(pa ? k0 : k1, pb ? k1 : kp2);
-            const float2 sa3 = make_float2(pa ? k1 : k0, pb ? kp2 : k1);
-            const float2 sa4 = make_float2(pa ? kp2 : km1, pb ? kp3 : k0);
-            float2 Fab = weno5_2(sa0, sa1, sa2, sa3, sa4);
+            float2 Fab;
+            // the kappa velocity's sign depends on the cell and direction only, so a warp's faces are
+            // usually all upwinded the same way: stencils in order then, per-element selects otherwise
+            if (__all_sync(FULL, pa && pb)) {
+                Fab = weno5_2(make_float2(km2, km1), make_float2(km1, k0), make_float2(k0, k1), make_float2(k1, kp2),
+                              make_float2(kp2, kp3));
+            } else if (__all_sync(FULL, !pa && !pb)) {
+                Fab = weno5_2(make_float2(kp3, kp4), make_float2(kp2, kp3), make_float2(k1, kp2), make_float2(k0, k1),
+                              make_float2(km1, k0));
+            } else {
+                const float2 sa0 = make_float2(pa ? km2 : kp3, pb ? km1 : kp4);
+                const float2 sa1 = make_float2(pa ? km1 : kp2, pb ? k0 : kp3);
+                const float2 sa2 = make_float2(pa ? k0 : k1, pb ? k1 : kp2);
+                const float2 sa3 = make_float2(pa ? k1 : k0, pb ? kp2 : k1);
+                const float2 sa4 = make_float2(pa ? kp2 : km1, pb ? kp3 : k0);
+                Fab = weno5_2(sa0, sa1, sa2, sa3, sa4);
+            }
             Fab.x = ha ? Fab.x : (pa ? k0 : k1);
             Fab.y = hb ? Fab.y : (pb ? k1 : kp2);
             // the - face of cell m0+1 is face a: recompute if cell m0+1 upwinds the other way
@@ -295,8 +339,11 @@ __device__ __forceinline__ void tile_body(const TileArgs& p, int tile, float* sm
             const float2 fk = mul2(make_float2(fk0, fk1), f2(dk_inv));
             // phi: window
             const bool qx = cp.x >= 0.f, qy = cp.y >= 0.f;
-            const float2 Fpp = weno5_2(sel2(qx, qy, w1, w6), sel2(qx, qy, w2, w5), sel2(qx, qy, w3, w4),
-                                       sel2(qx, qy, w4, w3), sel2(qx, qy, w5, w2));
+            float2 Fpp;
+            if (__all_sync(FULL, qx && qy)) Fpp = weno5_2(w1, w2, w3, w4, w5);   // same for the phi window
+            else if (__all_sync(FULL, !qx && !qy)) Fpp = weno5_2(w6, w5, w4, w3, w2);
+            else Fpp = weno5_2(sel2(qx, qy, w1, w6), sel2(qx, qy, w2, w5), sel2(qx, qy, w3, w4),
+                               sel2(qx, qy, w4, w3), sel2(qx, qy, w5, w2));
             float2 Fpm = prevF;
             if (!have || prevx != qx || prevy != qy) {
                 const float2 t = weno5_2(sel2(qx, qy, w0, w5), sel2(qx, qy, w1, w4), sel2(qx, qy, w2, w3),
@@ -311,9 +358,10 @@ __device__ __forceinline__ void tile_body(const TileArgs& p, int tile, float* sm
             const float2 fp = mul2(mul2(cp, sub2(Fpp, Fpm)), f2(dp_inv));
             G = mul2(f2(-1.f), add2(add2(add2(fx, fy), fk), fp));
         } else {
-            const float2 fx = mul2(flux2(V(-3, m0), V(-2, m0), V(-1, m0), c, V(1, m0), V(2, m0), V(3, m0), ux), f2(dx_inv));
-            const float2 fy = mul2(flux2(V(-3 * RW, m0), V(-2 * RW, m0), V(-RW, m0), c, V(RW, m0), V(2 * RW, m0),
-                                         V(3 * RW, m0), uy), f2(dy_inv));
+            float2 fx, fy;
+            flux_xy(V1, RW, c, ux, uy, fx, fy);
+            fx = mul2(fx, f2(dx_inv));
+            fy = mul2(fy, f2(dy_inv));
             G = mul2(f2(-1.f), add2(fx, fy));
         }
         if constexpr (SRC != 0) {
@@ -347,12 +395,22 @@ __device__ __forceinline__ void tile_body(const TileArgs& p, int tile, float* sm
     asm volatile("cp.async.wait_group 0;");
 }
 
-// Single-model kernel: 8 x 4 tiles, one CTA per tile.
-template <int L, bool REFRACT, int SRC>
-__global__ void __launch_bounds__(8 * 4 * L, 1) tile_kernel(const TileArgs p) {
+// Single-model kernel: one CTA per TX x TY tile, MINB CTAs resident per SM.
+template <int L, int TX, int TY, int MINB, bool REFRACT, int SRC>
+__global__ void __launch_bounds__(TX * TY * L, MINB) tile_kernel(const TileArgs p) {
     extern __shared__ __align__(16) float smem[];
-    tile_body<L, 8, 4, REFRACT, SRC>(p, blockIdx.x, smem);
+    tile_body<L, TX, TY, REFRACT, SRC>(p, blockIdx.x, smem);
 }
+
+// Tile shape of the single-model kernel per lane count: 256 threads and two CTAs per SM (while one CTA
+// waits at its per-plane barrier the other issues). Measured on seamount 1024^2 x 32 x 36 (stage 2):
+// 4 x 4 tiles 14.4 ms against 15.6 ms for one 512-thread CTA per SM with 8 x 4 tiles; 8 x 2 and 2 x 8
+// tiles, 128-thread CTAs four per SM, and three 256-thread CTAs per SM (96 registers, spilling) were
+// slower.
+template <int L> struct Shape;
+template <> struct Shape<16> { static constexpr int TX = 4, TY = 4, MINB = 2; };
+template <> struct Shape<8> { static constexpr int TX = 8, TY = 4, MINB = 2; };
+template <> struct Shape<4> { static constexpr int TX = 8, TY = 8, MINB = 2; };
 
 // Ensemble kernel: a persistent grid of ENSEMBLE_THREADS-thread CTAs takes work items (member, tile,
 // tile shape) from one atomic counter until the list is exhausted; no CTA ever waits for another.
@@ -392,16 +450,18 @@ __global__ void __launch_bounds__(ENSEMBLE_THREADS, 1)
 
 template <int L, bool REFRACT, int SRC>
 cudaError_t launch_variant(const TileArgs& a, int tiles, cudaStream_t s) {
-    const size_t smem = tile_smem_bytes(L, 8, 4);
-    auto k = tile_kernel<L, REFRACT, SRC>;
+    constexpr int TX = Shape<L>::TX, TY = Shape<L>::TY;
+    const size_t smem = tile_smem_bytes(L, TX, TY);
+    auto k = tile_kernel<L, TX, TY, Shape<L>::MINB, REFRACT, SRC>;
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k<<<tiles, 8 * 4 * L, smem, s>>>(a);
+    k<<<tiles, TX * TY * L, smem, s>>>(a);
     return cudaGetLastError();
 }
 
 template <int L>
 cudaError_t launch_L(const Handle& h, const StageParams& p, const TileArgs& a, cudaStream_t s) {
-    const int tiles = (int)(((h.desc.Nx + 7) / 8) * ((p.j_hi - p.j_lo + 3) / 4));
+    constexpr int TX = Shape<L>::TX, TY = Shape<L>::TY;
+    const int tiles = (int)(((h.desc.Nx + TX - 1) / TX) * ((p.j_hi - p.j_lo + TY - 1) / TY));
     const bool refract = p.transport == RPL_TRANSPORT_REFRACTION;
     const int src = p.learned ? 2 : ((p.has_wind || p.has_diss) ? 1 : (p.lin_rates ? 3 : 0));
     if (refract) {

@@ -190,10 +190,14 @@ def test_learned_stage_outputs_are_the_network_on_the_stage_input(torch):
     net.close()
 
 
-def test_learned_source_trained_beats_no_sources_and_flags_ood(torch):
-    """Train on plain-source states of a small hurricane, run it with the learned source: its Hs is much
-    closer to the plain run's than a run without sources or with the untrained network; cells with an
-    out-of-range wind fall back to the plain sources."""
+LEARNED_HS_TOL = 0.45
+
+
+def test_learned_source_error_against_the_plain_sources(torch):
+    """Train on plain-source states of a small hurricane (16 kappa x 24 directions, 4000 Adam steps), run
+    40 steps with the learned source: its Hs stays within rel-L2 LEARNED_HS_TOL of the plain-source run
+    (measured on B200: 0.33; without sources or with the untrained network the error is 1.0), and cells
+    with an out-of-range wind fall back to the plain sources."""
     w = small_storm()
     nb = 16 * 24
     net = learned.SourceNetwork(nbins=nb, hidden=256, rows=2048, seed=2)
@@ -226,6 +230,7 @@ def test_learned_source_trained_beats_no_sources_and_flags_ood(torch):
             assert learned.fallback_cells(mm) < P // 4
     err = {k: np.linalg.norm(Hs[k] - Hs["plain"]) / np.linalg.norm(Hs["plain"]) for k in Hs}
     print("Hs rel-L2 errors vs plain:", err)
+    assert err["learned"] <= LEARNED_HS_TOL, err
     assert err["learned"] < 0.5 * err["none"] and err["learned"] < 0.5 * err["untrained"], err
     # out of distribution: a wind-speed band no cell has sends every cell to the plain path
     lo2, hi2 = lo.copy(), hi.copy()
