@@ -58,6 +58,9 @@ def parse():
                     help="absolute widening of the per-bin log-action input bounds beyond the training rows, in "
                          "feature units (x 4 in log N); a cell outside the bounds uses the plain sources "
                          "(--workload learned)")
+    ap.add_argument("--learned-gate", type=float, default=0.0,
+                    help="trust gate of the learned source: cells whose network rates exceed this fraction of "
+                         "the action per step use the plain sources (0: off; --workload learned)")
     ap.add_argument("--calm-fraction", type=float, default=0.05,
                     help="share of cells without source activity kept as training rows (--workload learned)")
     ap.add_argument("--members", type=int, default=64, help="ensemble members (--workload ensemble)")
@@ -742,12 +745,12 @@ def run_learned(args, rank, world, local_rank):
     for mode in ("plain", "learned"):
         warm = w.model("fp32", device=local_rank)     # warm-up on a throwaway copy
         if mode == "learned":
-            learned.use_learned_source(warm, net, lo, hi, ylo, yhi)
+            learned.use_learned_source(warm, net, lo, hi, ylo, yhi, gate=args.learned_gate)
         rp.time_step(warm, w.dt, args.warmup)
         warm.close()
         m = w.model("fp32", device=local_rank)
         if mode == "learned":
-            learned.use_learned_source(m, net, lo, hi, ylo, yhi)
+            learned.use_learned_source(m, net, lo, hi, ylo, yhi, gate=args.learned_gate)
         lib, h = m._lib, m.handle
         stream = torch.cuda.Stream(device=local_rank)
         _lib.check(lib.rpl_set_stream(h, _lib.ctypes.c_void_p(stream.cuda_stream)))
@@ -812,7 +815,7 @@ def run_learned(args, rank, world, local_rank):
                        "total_action_rel_diff": abs(a["total"] - b["total"]) / b["total"],
                        "fallback_cells_last_stage": a["fallback"], "cells": P,
                        "training_rows": rows, "training_steps": args.train_steps * (2 + args.dagger) // 2,
-                       "dagger_rounds": args.dagger, "feature_pad": args.feature_pad, "training_s": t_train,
+                       "dagger_rounds": args.dagger, "feature_pad": args.feature_pad, "learned_gate": args.learned_gate, "training_s": t_train,
                        "data_generation_s": t_data, "losses": losses,
                        "mlp_forward_ms_per_stage": fwd_ms, "mlp_forward_tflops": flops / fwd_ms / 1e9,
                        "mlp_tensor_frac": flops / fwd_ms / 1e9 / bf16_peak, "bf16_peak_tflops": bf16_peak,

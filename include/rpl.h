@@ -410,6 +410,10 @@ int rpl_learned_sample(rpl_handle* h, const rpl_mlp* m, void* X, float* E, float
  * training targets keeps an extrapolating network from producing rates no source ever had). */
 int rpl_set_learned_source(rpl_handle* h, rpl_mlp* m, const float* lo, const float* hi, const float* ylo,
                            const float* yhi);
+/* Trust gate of the learned source (no counterpart in the reference): a cell whose network rates would
+ * change some bin by more than max_rate_dt of itself in one step (|rate| * dt > max_rate_dt) takes the
+ * plain sources for that stage, like an out-of-distribution cell. 0 (the default) disables the gate. */
+int rpl_set_learned_gate(rpl_handle* h, double max_rate_dt);
 /* Network outputs y of the most recent stage (host, Nx*Ny rows of nbins, row c = cell i + Nx j). */
 int rpl_learned_outputs(rpl_handle* h, float* Y);
 /* Cells that fell back to the plain sources in the most recent stage. */

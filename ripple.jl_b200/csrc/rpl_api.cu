@@ -151,7 +151,7 @@ int launch_stage_rows(Handle* h, double dt, int stage, int64_t j_lo, int64_t j_h
     if (prepare) {
         if (sources) {
             if (stage == 1) RPL_CUDA(rpl::launch_wind(*h, h->time, s));
-            if (h->learned) RPL_CUDA(rpl::launch_learned_stage_prep(*h, Nin, s));
+            if (h->learned) RPL_CUDA(rpl::launch_learned_stage_prep(*h, Nin, dt, s));
             else if (h->src.stress_cap) RPL_CUDA(rpl::launch_stress_factor(*h, Nin, s));
         }
         if (h->pm) RPL_CUDA(rpl::launch_pm_refresh(*h, Nin, s, false));

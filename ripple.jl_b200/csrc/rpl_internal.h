@@ -138,6 +138,7 @@ struct Handle {
     float* d_lbounds = nullptr;    // lo[nbins + 4], hi[nbins + 4]
     int64_t lrows = 0;
     bool lclamp = false;           // clamp the network outputs to the output bounds
+    double lgate = 0.0;            // > 0: a cell whose network rates have |rate| * dt above it uses the plain sources
     bool currents_set = false;
     // prescribed currents: the Q grid and the last currents stay on the device so the coupling can be
     // refreshed (rpl_update_currents*) without allocating
@@ -197,7 +198,7 @@ struct Handle {
 // Learned-source network internals (rpl_mlp.cu, rpl_learned.cu).
 int mlp_nbins(const rpl_mlp* m);
 const rpl_mlp_desc& mlp_desc(const rpl_mlp* m);
-cudaError_t launch_learned_stage_prep(const Handle& h, const void* Nin, cudaStream_t s);
+cudaError_t launch_learned_stage_prep(const Handle& h, const void* Nin, double dt, cudaStream_t s);
 void free_learned(Handle* h);
 
 // Pseudomomentum self-coupling (rpl_pm.cu): refresh the velocity and coefficient records from the

@@ -3,8 +3,9 @@
 // Per stage (rpl_api.cu launch_step): the feature kernel turns the stage input into network rows (per
 // cell: the Nk*Np BF16 log-action features in bin order m + Nk n, and 4 extras) and flags every cell
 // with an input outside the training bounds; the stress cap runs for flagged cells only; the network
-// (rpl_mlp.cu) writes the per-bin outputs y; the tile kernel adds N * target_scale * sinh(y), or the
-// plain FP32 sources for flagged cells. rpl_learned_sample writes the same rows plus the plain sources'
+// (rpl_mlp.cu) writes the per-bin outputs y; with a trust gate (rpl_set_learned_gate) cells whose network
+// rates are stiff are flagged too; the stress cap runs for flagged cells; the tile kernel adds
+// N * target_scale * sinh(y), or the plain FP32 sources for flagged cells. rpl_learned_sample writes the same rows plus the plain sources'
 // rates as targets, in the network's output form asinh(rate / target_scale) (relative accuracy uniform
 // over the rates' decades). Reference for the replaced terms: precomputed_sources.jl:396-439,
 // pressure_correlation.jl:109-156, local_saturation.jl:30-47.
@@ -83,6 +84,20 @@ __global__ void rows_kernel(const RowArgs a, const StageParams p) {
     if (!SAMPLE && __any_sync(0xffffffffu, bad) && lane == 0) atomicOr(a.flag + c, 1u);
 }
 
+// Trust gate of the network: one warp per cell over its bins; a cell whose network rate would change any
+// bin by more than `gate` of itself in one step (|lscale sinh(y)| * dt > gate) is flagged and takes the
+// plain sources instead. Stiff cells are where a rate error compounds fastest from step to step.
+__global__ void gate_kernel(const float* __restrict__ Y, int64_t P, int nb, float lscale, float limit,
+                            unsigned int* flag) {
+    const int64_t c = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (c >= P) return;  // uniform per warp
+    float big = 0.0f;
+    for (int b = lane; b < nb; b += 32) big = fmaxf(big, fabsf(__ldg(Y + c * nb + b)));
+    for (int o = 16; o > 0; o >>= 1) big = fmaxf(big, __shfl_xor_sync(0xffffffffu, big, o));
+    if (lane == 0 && lscale * sinhf(big) > limit) atomicOr(flag + c, 2u);
+}
+
 RowArgs row_args(const Handle& h, const rpl_mlp_desc& md, const void* Nin) {
     RowArgs a{};
     a.N = (const float*)Nin;
@@ -115,7 +130,7 @@ int check_learned_handle(const Handle& h, const rpl_mlp* m) {
 
 }  // namespace
 
-cudaError_t launch_learned_stage_prep(const Handle& h, const void* Nin, cudaStream_t s) {
+cudaError_t launch_learned_stage_prep(const Handle& h, const void* Nin, double dt, cudaStream_t s) {
     const rpl_mlp_desc& md = mlp_desc(h.learned);
     RowArgs a = row_args(h, md, Nin);
     a.X = (bf16*)h.d_lx;
@@ -128,11 +143,19 @@ cudaError_t launch_learned_stage_prep(const Handle& h, const void* Nin, cudaStre
     const StageParams p = make_params(h, 1.0, 1);
     rows_kernel<false><<<blocks_for_warps(h.cells * h.desc.Np), 256, 0, s>>>(a, p);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    if (h.src.stress_cap && (e = launch_stress_factor(h, Nin, s, h.d_lflag)) != cudaSuccess) return e;
     const int nb = mlp_nbins(h.learned);
     const float* ylo = h.lclamp ? h.d_lbounds + 2 * (nb + 4) : nullptr;
-    return mlp_forward(h.learned, (const bf16*)h.d_lx, nb, h.d_le, h.lrows, h.d_lr, nb, false, s, h.d_err, ylo,
-                       ylo ? ylo + nb : nullptr);
+    e = mlp_forward(h.learned, (const bf16*)h.d_lx, nb, h.d_le, h.lrows, h.d_lr, nb, false, s, h.d_err, ylo,
+                    ylo ? ylo + nb : nullptr);
+    if (e != cudaSuccess) return e;
+    if (h.lgate > 0.0) {
+        gate_kernel<<<blocks_for_warps(h.cells), 256, 0, s>>>(h.d_lr, h.cells, nb, md.target_scale,
+                                                              (float)(h.lgate / dt), h.d_lflag);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    // the stress cap of the plain sources, for the cells that take them
+    if (h.src.stress_cap) e = launch_stress_factor(h, Nin, s, h.d_lflag);
+    return e;
 }
 
 void free_learned(Handle* h) {
@@ -225,6 +248,14 @@ int rpl_set_learned_source(rpl_handle* hh, rpl_mlp* m, const float* lo, const fl
     h->learned = m;
     h->lrows = rows;
     h->lclamp = ylo != nullptr;
+    return RPL_OK;
+}
+
+int rpl_set_learned_gate(rpl_handle* hh, double max_rate_dt) {
+    if (!hh) return rpl::lfail(RPL_ERR_ARGUMENT, "null handle");
+    if (!(max_rate_dt >= 0.0) || !std::isfinite(max_rate_dt))
+        return rpl::lfail(RPL_ERR_ARGUMENT, "the gate must be a finite value >= 0 (0: no gate)");
+    reinterpret_cast<Handle*>(hh)->lgate = max_rate_dt;
     return RPL_OK;
 }
 

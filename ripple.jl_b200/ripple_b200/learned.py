@@ -114,10 +114,11 @@ def sample(model, net, out=None):
     return X, E, T
 
 
-def use_learned_source(model, net, lo=None, hi=None, ylo=None, yhi=None):
+def use_learned_source(model, net, lo=None, hi=None, ylo=None, yhi=None, gate=0.0):
     """Replace the model's plain sources by `net` (None: back to the plain sources). lo, hi: input bounds
     (nbins + 4 values); a cell with any input outside them uses the plain sources. ylo, yhi (optional,
-    nbins values): the network's outputs are clamped to them (see output_bounds)."""
+    nbins values): the network's outputs are clamped to them (see output_bounds). gate > 0: a cell whose
+    network rates would change a bin by more than `gate` of itself in one step uses the plain sources too."""
     if net is None:
         check(model._lib.rpl_set_learned_source(model.handle, None, None, None, None, None))
         return
@@ -134,6 +135,7 @@ def use_learned_source(model, net, lo=None, hi=None, ylo=None, yhi=None):
         yp = [ctypes.c_void_p(ylo.ctypes.data), ctypes.c_void_p(yhi.ctypes.data)]
     check(model._lib.rpl_set_learned_source(model.handle, net.handle, ctypes.c_void_p(lo.ctypes.data),
                                             ctypes.c_void_p(hi.ctypes.data), *yp))
+    check(model._lib.rpl_set_learned_gate(model.handle, float(gate)))
     model._learned_keep = (net, lo, hi, ylo, yhi)
 
 

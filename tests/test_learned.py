@@ -241,3 +241,24 @@ def test_learned_source_error_against_the_plain_sources(torch):
     assert learned.fallback_cells(mm) == P
     untrained.close()
     net.close()
+
+
+def test_learned_trust_gate(torch):
+    """The trust gate: with a gate no rate reaches the run equals the ungated learned run bit for bit; a
+    small gate sends the cells with stiff network rates to the plain sources."""
+    w = small_storm(nsteps=1)
+    nb = 16 * 24
+    net = learned.SourceNetwork(nbins=nb, hidden=256, rows=2048, seed=2)
+    lo, hi = np.full(nb + 4, -1e9, np.float32), np.full(nb + 4, 1e9, np.float32)
+    res = {}
+    for name, gate in (("none", 0.0), ("huge", 1e30), ("small", 1e-6)):
+        m = w.model("fp32")
+        rp.time_step(m, w.dt, 3)
+        learned.use_learned_source(m, net, lo, hi, gate=gate)
+        rp.time_step(m, w.dt, 2)
+        res[name] = (m.action.interior().copy(), learned.fallback_cells(m))
+        m.close()
+    assert np.array_equal(res["none"][0], res["huge"][0]) and res["none"][1] == res["huge"][1] == 0
+    assert res["small"][1] > 0
+    assert not np.array_equal(res["small"][0], res["none"][0])
+    net.close()
