@@ -284,41 +284,36 @@ diag_kernel(const T* __restrict__ N, int64_t Nx, int64_t Ny, int64_t Nk, int64_t
     const int nk = (int)Nk, np = (int)Np;
     for (int m = lane; m < nk; m += 32) {
         const T* p = N + c * Nk + m;
-        // blocks of DB directions: the block's loads are issued together, its terms summed with FMAs,
-        // and the block sum folded into the compensated totals
-        constexpr int DB = 4;
-        auto block = [&](int n0, const T* q) {
-            double a[DB];
-            int b[DB];
+        // chunks of CH directions: the chunk's loads are issued together (memory-level parallelism), then
+        // its blocks of DB directions are summed with FMAs and each block sum is folded into the
+        // compensated totals, block by block in direction order
+        constexpr int DB = 4, CH = 3 * DB;
+        for (int n0 = 0; n0 < np; n0 += CH, p += CH * stride) {
+            T a[CH];
 #pragma unroll
-            for (int k = 0; k < DB; ++k) {
-                const bool in = n0 + k < np;
-                a[k] = in ? (double)q[k * stride] : 0.0;
-                b[k] = in ? m + nk * (n0 + k) : m;  // a[k] = 0 past the last direction
-            }
-            double b0 = 0.0, bx = 0.0, by = 0.0, bt = 0.0;
+            for (int k = 0; k < CH; ++k) a[k] = n0 + k < np ? p[k * stride] : T(0);
 #pragma unroll
-            for (int k = 0; k < DB; ++k) {
-                b0 = fma(a[k], __ldg(w + b[k]), b0);
+            for (int q = 0; q < CH; q += DB) {
+                if (n0 + q >= np) break;
+                double b0 = 0.0, bx = 0.0, by = 0.0, bt = 0.0;
+#pragma unroll
+                for (int k = q; k < q + DB; ++k) {
+                    const int b = n0 + k < np ? m + nk * (n0 + k) : m;  // a[k] = 0 past the last direction
+                    const double ak = (double)a[k];
+                    b0 = fma(ak, __ldg(w + b), b0);
+                    if (ALL) {
+                        bx = fma(ak, __ldg(mux + b), bx);
+                        by = fma(ak, __ldg(muy + b), by);
+                        bt = fma(ak, __ldg(tr + b), bt);
+                    }
+                }
+                tadd(s0, c0, b0);
                 if (ALL) {
-                    bx = fma(a[k], __ldg(mux + b[k]), bx);
-                    by = fma(a[k], __ldg(muy + b[k]), by);
-                    bt = fma(a[k], __ldg(tr + b[k]), bt);
+                    tadd(sx, cx, bx);
+                    tadd(sy, cy, by);
+                    tadd(st, ct, bt);
                 }
             }
-            tadd(s0, c0, b0);
-            if (ALL) {
-                tadd(sx, cx, bx);
-                tadd(sy, cy, by);
-                tadd(st, ct, bt);
-            }
-        };
-        if (ALL) {
-            for (int n0 = 0; n0 < np; n0 += DB, p += DB * stride) block(n0, p);
-        } else {
-            // m0 alone has registers to spare: two blocks' loads in flight, the same summation order
-#pragma unroll 2
-            for (int n0 = 0; n0 < np; n0 += DB, p += DB * stride) block(n0, p);
         }
     }
 #pragma unroll
