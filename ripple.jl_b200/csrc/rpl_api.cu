@@ -77,7 +77,7 @@ void free_all(Handle* h) {
     rpl::free_currents(h);
     void* ptrs[] = {h->N, h->A, h->B, h->d_kappa, h->d_phi, h->d_cos, h->d_sin, h->d_weights, h->d_cgx,
                     h->d_cgy, h->d_cgmag, h->d_depth, h->d_coupling, h->d_wind, h->d_diag, h->d_err,
-                    h->d_coef, h->d_tab32, h->d_cell32, h->d_bin32, h->d_U, h->d_spacing};
+                    h->d_coef, h->d_tab32, h->d_cell32, h->d_bin32, h->d_U, h->d_spacing, h->d_sxy};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->h_err) cudaFreeHost(h->h_err);
@@ -258,7 +258,8 @@ int rpl_create(const rpl_desc* d, rpl_handle** out) {
     const size_t elem = d->precision == RPL_FP64 ? 8 : 4;
     const int64_t c3 = d->Nx * d->Ny * d->Nk, P = d->Nx * d->Ny, nb = d->Nk * d->Np;
     int64_t need = 3 * units * (int64_t)elem + 16 * c3 * 8 + (d->depth_kind == RPL_DEPTH_FIELD ? (c3 + P) * 8 : 0) +
-                   (4 * P + 2 * (d->Nx + d->Ny)) * 8 + 6 * P * 8 + 8 * nb * 8;
+                   (4 * P + 2 * (d->Nx + d->Ny)) * 8 + 6 * P * 8 + 8 * nb * 8 +
+                   (d->precision == RPL_FP32 && d->transport == RPL_TRANSPORT_REFRACTION ? units * 4 : 0);
     if (d->memory_limit_bytes > 0 && need > d->memory_limit_bytes)
         return fail(RPL_ERR_OOM, "model needs " + std::to_string(need) + " device bytes, above the memory limit of " +
                                      std::to_string(d->memory_limit_bytes));
@@ -389,6 +390,8 @@ int rpl_create(const rpl_desc* d, rpl_handle** out) {
     TRY(dalloc(h, &h->d_coef, 8 * c3));
     TRY(dalloc(h, &h->d_cell32, 8 * P));
     TRY(dalloc(h, &h->d_bin32, 8 * d->Nk));
+    if (d->transport == RPL_TRANSPORT_REFRACTION && rpl::tile32_supported(*h) && !h->force_column_kernel)
+        TRY(dalloc(h, &h->d_sxy, units));  // the two-pass refraction stage of FP32 models
     TRY(rpl::launch_coef(*h, s));
     {
         std::vector<float> tab32(6 * d->Np + 3 * nb);

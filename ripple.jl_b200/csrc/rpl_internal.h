@@ -83,6 +83,7 @@ struct TileArgs {
     int learned, pad1;
     const float* lin_rates;  // SourceTermSet rates per cell-bin (state layout) or null
     int j_lo, j_hi;          // rows the stage updates
+    float* sxy;              // two-pass refraction stage: x+y flux sums per cell-bin (state layout), or null
 };
 
 // Tile shapes (kappa-pair lanes per cell L, tile TX x TY) compiled into the ensemble kernel; every
@@ -129,6 +130,7 @@ struct Handle {
     float* d_tab32 = nullptr;      // FP32 copies: 4*Np trig, 2*Nk*Np group velocity, 2*Np cos/sin, Nk*Np weights
     float* d_cell32 = nullptr;     // (Nx*Ny) x 8 floats of per-cell wind constants
     float* d_bin32 = nullptr;      // Nk x 8 floats of per-kappa source constants
+    float* d_sxy = nullptr;        // FP32 refraction models: x+y flux sums between the two stage passes
     // learned source (rpl_learned.cu)
     rpl_mlp* learned = nullptr;
     void* d_lx = nullptr;          // (rows x nbins) BF16 features, rows = cells rounded up to 128

@@ -395,6 +395,259 @@ __device__ __forceinline__ void tile_body(const TileArgs& p, int tile, float* sm
     asm volatile("cp.async.wait_group 0;");
 }
 
+// Refraction stages of FP32 models run as two kernels with smaller register footprints than the fused
+// tile body, so more warps hide the latency of the WENO5 chains (measured on seamount 1024^2 x 32 x 36:
+// 12.9 ms per stage against 14.4 ms fused, bit-identical results):
+//   xy_kernel (pass A): the tile body's staging of the phi planes and its x and y fluxes; writes
+//     S = fx/dx + fy/dy per cell-bin (state layout);
+//   kp_kernel (pass B): one thread per (cell, kappa pair) walking the phi ring with its register window,
+//     the kappa stencil from the cell's other lanes (warp shuffles, the reference's clamped indices),
+//     the kappa and phi fluxes, sources and the stage update: G = -(((S + fk) + fp)), the fused kernel's
+//     order of additions.
+template <int L, int TX, int TY>
+__device__ __forceinline__ void xy_body(const TileArgs& p, int tile, float* smem) {
+    float* S = p.sxy;
+    constexpr int RW = TX + 6, RH = TY + 6, KP = 2 * L, THREADS = TX * TY * L, CROSS = RW * TY + 6 * TX;
+    const float* __restrict__ Nin = p.Nin;
+    const int Nx = p.Nx, Ny = p.Ny, Nk = p.Nk, Np = p.Np;
+    const int64_t slice = (int64_t)Nx * Ny * Nk;
+    const int tiles_x = (Nx + TX - 1) / TX;
+    const int i0 = (tile % tiles_x) * TX, j0 = p.j_lo + (tile / tiles_x) * TY;
+    const int tid = threadIdx.x, l = tid % L, cell = tid / L, cx = cell % TX, cy = cell / TX;
+    const int i = i0 + cx, j = j0 + cy;
+    const bool live_cell = i < Nx && j < p.j_hi;
+    const int ic = i < Nx ? i : Nx - 1, jc = j < p.j_hi ? j : p.j_hi - 1;
+    const int m0 = 2 * l;
+    const bool live = live_cell && m0 < Nk;
+    const int mc = m0 < Nk ? m0 : Nk - 2;
+    const int64_t home = ((int64_t)jc * Nx + ic) * Nk + mc;
+    const int KC = Nk / 4, nchunks = CROSS * KC;
+    constexpr int MAXC = (CROSS * (KP / 4) + THREADS - 1) / THREADS;
+    int64_t goff[MAXC];
+    int soff[MAXC];
+#pragma unroll
+    for (int k = 0; k < MAXC; ++k) {
+        const int q = tid + k * THREADS;
+        goff[k] = -1;
+        soff[k] = 0;
+        if (q < nchunks) {
+            const int col = q / KC, part = q % KC;
+            int dx, dy;
+            if (col < RW * TY) { dy = col / RW; dx = col % RW - 3; }
+            else { const int r = col - RW * TY, yi = r / TX; dx = r % TX; dy = yi < 3 ? yi - 3 : TY + yi - 3; }
+            int gi = i0 + dx, gj = j0 + dy;
+            gi = gi < 0 ? gi + Nx : (gi >= Nx ? gi - Nx : gi);
+            gj = gj < 0 ? gj + Ny : (gj >= Ny ? gj - Ny : gj);
+            gi = gi < 0 ? 0 : (gi >= Nx ? Nx - 1 : gi);
+            gj = gj < 0 ? 0 : (gj >= Ny ? Ny - 1 : gj);
+            goff[k] = ((int64_t)gj * Nx + gi) * Nk + 4 * part;
+            soff[k] = ((dy + 3) * RW + (dx + 3)) * KP + 4 * part;
+        }
+    }
+    const int plane_floats = RW * RH * KP;
+    auto issue = [&](int n) {
+        if (n < Np) {
+            float* buf = smem + (n % NB) * plane_floats;
+            const float* src = Nin + slice * n;
+#pragma unroll
+            for (int k = 0; k < MAXC; ++k)
+                if (goff[k] >= 0) {
+                    const unsigned sa = (unsigned)__cvta_generic_to_shared(buf + soff[k]);
+                    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(src + goff[k]));
+                }
+        }
+        asm volatile("cp.async.commit_group;");
+    };
+    issue(0);
+    issue(1);
+    const double* rec0 = p.coef + 8 * (((int64_t)jc * Nx + ic) * Nk + mc);
+    const double* rec1 = rec0 + 8;
+    const float2 Ux = make_float2((float)rec0[0], (float)rec1[0]), Uy = make_float2((float)rec0[1], (float)rec1[1]);
+    const float2 cgm = make_float2((float)rec0[6], (float)rec1[6]);
+    const float dx_inv = p.dx_inv, dy_inv = p.dy_inv;
+    const int ctr = ((cy + 3) * RW + (cx + 3)) * KP;
+    for (int n = 0; n < Np; ++n) {
+        asm volatile("cp.async.wait_group 1;");
+        __syncthreads();
+        issue(n + 2);
+        const float* pl = smem + (n % NB) * plane_floats + ctr;
+        auto V1 = [&](int dcol) { return *reinterpret_cast<const float2*>(pl + dcol * KP + mc); };
+        const float2 c = *reinterpret_cast<const float2*>(pl + mc);
+        const float4 g = __ldg(reinterpret_cast<const float4*>(p.cg32 + mc + Nk * n));
+        float2 ux = make_float2(g.x, g.z), uy = make_float2(g.y, g.w);
+        if (p.cg_per_cell) {
+            ux = mul2(cgm, ux);
+            uy = mul2(cgm, uy);
+        }
+        ux = add2(ux, Ux);
+        uy = add2(uy, Uy);
+        float2 fx, fy;
+        flux_xy(V1, RW, c, ux, uy, fx, fy);
+        fx = mul2(fx, f2(dx_inv));
+        fy = mul2(fy, f2(dy_inv));
+        if (live) *reinterpret_cast<float2*>(S + slice * n + home) = add2(fx, fy);
+    }
+    asm volatile("cp.async.wait_group 0;");
+}
+
+
+template <int L, int TX, int TY, int MINB>
+__global__ void __launch_bounds__(TX * TY * L, MINB) xy_kernel(const TileArgs p) {
+    extern __shared__ __align__(16) float smem[];
+    xy_body<L, TX, TY>(p, blockIdx.x, smem);
+}
+
+// Pass B: one thread per (cell, kappa pair), CPB cells per CTA, no shared memory.
+template <int L, int CPB, int MINB, int SRC>
+__global__ void __launch_bounds__(CPB * L, MINB) kp_kernel(const TileArgs p) {
+    const float* __restrict__ S = p.sxy;
+    const float* __restrict__ Nin = p.Nin;
+    const float* N0 = p.N0;
+    float* Nout = p.Nout;
+    const int Nx = p.Nx, Ny = p.Ny, Nk = p.Nk, Np = p.Np;
+    const int64_t slice = (int64_t)Nx * Ny * Nk;
+    const int64_t P = (int64_t)Nx * (p.j_hi - p.j_lo);
+    const int tid = threadIdx.x, l = tid % L;
+    const int64_t cidx = (int64_t)blockIdx.x * CPB + tid / L;
+    const bool live_cell = cidx < P;
+    const int64_t cc = (live_cell ? cidx : P - 1) + (int64_t)Nx * p.j_lo;
+    const int m0 = 2 * l;
+    const bool live = live_cell && m0 < Nk;
+    const int mc = m0 < Nk ? m0 : Nk - 2;
+    const int64_t home = cc * Nk + mc;
+    const double* rec0 = p.coef + 8 * (cc * Nk + mc);
+    const double* rec1 = rec0 + 8;
+    const float2 kap = make_float2((float)rec0[7], (float)rec1[7]);
+    const float2 Uxx = make_float2((float)rec0[2], (float)rec1[2]), Uxy = make_float2((float)rec0[3], (float)rec1[3]);
+    const float2 Uyx = make_float2((float)rec0[4], (float)rec1[4]), Uyy = make_float2((float)rec0[5], (float)rec1[5]);
+    // source constants of this cell and of the lane's two kappa bins (as the tile body)
+    Cell32 wc{};
+    Bin32 wb0{}, wb1{};
+    bool plain_src = SRC == 1;
+    const float* lrow = nullptr;
+    if constexpr (SRC == 1 || SRC == 2) {
+        wc = load_cell32(p.cell32 + 8 * cc);
+        wb0 = load_bin32(p.bin32 + 8 * mc);
+        wb1 = load_bin32(p.bin32 + 8 * (mc + 1));
+        if constexpr (SRC == 2) {
+            plain_src = __ldg(p.lflag + cc) != 0u;
+            lrow = p.lrate + cc * ((int64_t)Nk * Np) + mc;
+        }
+    }
+    const float2* own = reinterpret_cast<const float2*>(Nin + home);
+    const int64_t s2 = slice / 2;
+    auto wr = [&](int n) { return n < 0 ? n + Np : (n >= Np ? n - Np : n); };
+    float2 w0 = own[s2 * wr(-3)], w1 = own[s2 * wr(-2)], w2 = own[s2 * wr(-1)], w3 = own[0];
+    float2 w4 = own[s2 * wr(1)], w5 = own[s2 * wr(2)], w6 = own[s2 * wr(3)];
+    const float dk_inv = p.dk_inv, dp_inv = p.dp_inv, dt = p.dt, ca = p.a, cb = p.b;
+    const bool ha = (m0 - 2 >= 0) && (m0 + 3 <= Nk - 1);
+    const bool hb = (m0 - 1 >= 0) && (m0 + 4 <= Nk - 1);
+    const bool hlo = (m0 - 3 >= 0) && (m0 + 2 <= Nk - 1);
+    const bool up2 = m0 + 2 <= Nk - 1, up3 = m0 + 3 <= Nk - 1, up4 = m0 + 4 <= Nk - 1;
+    float2 prevF = f2(0.f);
+    bool prevx = false, prevy = false, have = false;
+    for (int n = 0; n < Np; ++n) {
+        const float2 nxt = own[s2 * ((n + 4) % Np)];
+        const float2 n0v = (p.stage == 1 || !live) ? f2(0.f) : *reinterpret_cast<const float2*>(N0 + slice * n + home);
+        const float2 sxy = *reinterpret_cast<const float2*>(S + slice * n + home);
+        const float2 c = w3;
+        const float4 tg = __ldg(p.trig32 + n);
+        const float2 ck = mul2(mul2(f2(-1.f), kap),
+                               add2(add2(mul2(f2(tg.x), Uxx), mul2(f2(tg.y), add2(Uyx, Uxy))), mul2(f2(tg.z), Uyy)));
+        const float2 cp = sub2(add2(mul2(f2(tg.y), sub2(Uxx, Uyy)), mul2(f2(tg.z), Uyx)), mul2(f2(tg.x), Uxy));
+        // kappa stencil of the lane's pair (the reference's clamped indices) from the neighbouring lanes
+        const float a_ = __shfl_sync(FULL, c.x, l - 1, L), b_ = __shfl_sync(FULL, c.y, l - 1, L);
+        const float d_ = __shfl_sync(FULL, c.y, l - 2, L);
+        const float e_ = __shfl_sync(FULL, c.x, l + 1, L), f_ = __shfl_sync(FULL, c.y, l + 1, L);
+        const float g_ = __shfl_sync(FULL, c.x, l + 2, L);
+        const float k0 = c.x, k1 = c.y;
+        const float km1 = l >= 1 ? b_ : k0, km2 = l >= 1 ? a_ : k0, km3 = l >= 2 ? d_ : (l == 1 ? a_ : k0);
+        const float kp2 = up2 ? e_ : k1, kp3 = up3 ? f_ : k1, kp4 = up4 ? g_ : (up3 ? f_ : k1);
+        const bool pa = ck.x >= 0.f, pb = ck.y >= 0.f;
+        float2 Fab;
+        if (__all_sync(FULL, pa && pb)) {
+            Fab = weno5_2(make_float2(km2, km1), make_float2(km1, k0), make_float2(k0, k1), make_float2(k1, kp2),
+                          make_float2(kp2, kp3));
+        } else if (__all_sync(FULL, !pa && !pb)) {
+            Fab = weno5_2(make_float2(kp3, kp4), make_float2(kp2, kp3), make_float2(k1, kp2), make_float2(k0, k1),
+                          make_float2(km1, k0));
+        } else {
+            const float2 sa0 = make_float2(pa ? km2 : kp3, pb ? km1 : kp4);
+            const float2 sa1 = make_float2(pa ? km1 : kp2, pb ? k0 : kp3);
+            const float2 sa2 = make_float2(pa ? k0 : k1, pb ? k1 : kp2);
+            const float2 sa3 = make_float2(pa ? k1 : k0, pb ? kp2 : k1);
+            const float2 sa4 = make_float2(pa ? kp2 : km1, pb ? kp3 : k0);
+            Fab = weno5_2(sa0, sa1, sa2, sa3, sa4);
+        }
+        Fab.x = ha ? Fab.x : (pa ? k0 : k1);
+        Fab.y = hb ? Fab.y : (pb ? k1 : kp2);
+        float Fam1 = Fab.x;
+        if (pa != pb) {
+            const float2 t = weno5_2(make_float2(pb ? km2 : kp3, 0.f), make_float2(pb ? km1 : kp2, 0.f),
+                                     make_float2(pb ? k0 : k1, 0.f), make_float2(pb ? k1 : k0, 0.f),
+                                     make_float2(pb ? kp2 : km1, 0.f));
+            Fam1 = ha ? t.x : (pb ? k0 : k1);
+        }
+        const float upF = __shfl_up_sync(FULL, Fab.y, 1, L);
+        const bool upP = __shfl_up_sync(FULL, (int)pb, 1, L) != 0;
+        float Flo = upF;
+        if (m0 >= 1 && upP != pa) {
+            const float2 t = weno5_2(make_float2(pa ? km3 : kp2, 0.f), make_float2(pa ? km2 : k1, 0.f),
+                                     make_float2(pa ? km1 : k0, 0.f), make_float2(pa ? k0 : km1, 0.f),
+                                     make_float2(pa ? k1 : km2, 0.f));
+            Flo = hlo ? t.x : (pa ? km1 : k0);
+        }
+        const float fk0 = ((m0 == Nk - 1) ? 0.f : ck.x * Fab.x) - ((m0 == 0) ? 0.f : ck.x * Flo);
+        const float fk1 = ((m0 + 1 == Nk - 1) ? 0.f : ck.y * Fab.y) - ck.y * Fam1;
+        const float2 fk = mul2(make_float2(fk0, fk1), f2(dk_inv));
+        const bool qx = cp.x >= 0.f, qy = cp.y >= 0.f;
+        float2 Fpp;
+        if (__all_sync(FULL, qx && qy)) Fpp = weno5_2(w1, w2, w3, w4, w5);
+        else if (__all_sync(FULL, !qx && !qy)) Fpp = weno5_2(w6, w5, w4, w3, w2);
+        else Fpp = weno5_2(sel2(qx, qy, w1, w6), sel2(qx, qy, w2, w5), sel2(qx, qy, w3, w4), sel2(qx, qy, w4, w3),
+                           sel2(qx, qy, w5, w2));
+        float2 Fpm = prevF;
+        if (!have || prevx != qx || prevy != qy) {
+            const float2 t = weno5_2(sel2(qx, qy, w0, w5), sel2(qx, qy, w1, w4), sel2(qx, qy, w2, w3),
+                                     sel2(qx, qy, w3, w2), sel2(qx, qy, w4, w1));
+            if (!have || prevx != qx) Fpm.x = t.x;
+            if (!have || prevy != qy) Fpm.y = t.y;
+        }
+        prevF = Fpp;
+        prevx = qx;
+        prevy = qy;
+        have = true;
+        const float2 fp = mul2(mul2(cp, sub2(Fpp, Fpm)), f2(dp_inv));
+        float2 G = mul2(f2(-1.f), add2(add2(sxy, fk), fp));
+        if constexpr (SRC != 0) {
+            if (plain_src) {
+                const float2 cs = __ldg(p.cs32 + n);
+                G.x += source32(p, wc, wb0, cs.x, cs.y, c.x);
+                G.y += source32(p, wc, wb1, cs.x, cs.y, c.y);
+            } else if (SRC == 2) {  // learned: N * rate, rate = lscale * sinh(network output of bin (m, n))
+                const float2 y = __ldg(reinterpret_cast<const float2*>(lrow + (int64_t)n * Nk));
+                G = fma2(mul2(c, f2(p.lscale)), make_float2(sinhf(y.x), sinhf(y.y)), G);
+            } else {  // SourceTermSet rates of this stage, state layout
+                G = fma2(*reinterpret_cast<const float2*>(p.lin_rates + slice * n + home), c, G);
+            }
+        }
+        float2 st = fma2(f2(dt), G, c);
+        st.x = relu(st.x);
+        st.y = relu(st.y);
+        float2 out = st;
+        if (p.stage != 1) {
+            out = fma2(f2(ca), n0v, mul2(f2(cb), st));
+            out.x = relu(out.x);
+            out.y = relu(out.y);
+        }
+        if (live) {
+            if (!isfinite(out.x) || !isfinite(out.y)) atomicOr(p.err, 1u);
+            *reinterpret_cast<float2*>(Nout + slice * n + home) = out;
+        }
+        w0 = w1; w1 = w2; w2 = w3; w3 = w4; w4 = w5; w5 = w6; w6 = nxt;
+    }
+}
+
 // Single-model kernel: one CTA per TX x TY tile, MINB CTAs resident per SM.
 template <int L, int TX, int TY, int MINB, bool REFRACT, int SRC>
 __global__ void __launch_bounds__(TX * TY * L, MINB) tile_kernel(const TileArgs p) {
@@ -458,12 +711,36 @@ cudaError_t launch_variant(const TileArgs& a, int tiles, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+// Two-pass refraction stage: pass A over the shape's tiles, then pass B over 256-thread CTAs, three CTAs
+// per SM each (24 warps at <= 80 registers).
+template <int L, int SRC>
+cudaError_t launch_split(const TileArgs& a, cudaStream_t s) {
+    constexpr int TX = Shape<L>::TX, TY = Shape<L>::TY, CPB = 256 / L;
+    const int tiles = ((a.Nx + TX - 1) / TX) * ((a.j_hi - a.j_lo + TY - 1) / TY);
+    const size_t smem = tile_smem_bytes(L, TX, TY);
+    auto ka = xy_kernel<L, TX, TY, 3>;
+    cudaFuncSetAttribute(ka, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    ka<<<tiles, TX * TY * L, smem, s>>>(a);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    const int64_t cells = (int64_t)a.Nx * (a.j_hi - a.j_lo);
+    // the per-cell source constants of the bundle and the learned source need registers: two CTAs per SM
+    constexpr int BMINB = (SRC == 1 || SRC == 2) ? 2 : 3;
+    kp_kernel<L, CPB, BMINB, SRC><<<(unsigned)((cells + CPB - 1) / CPB), CPB * L, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
 template <int L>
 cudaError_t launch_L(const Handle& h, const StageParams& p, const TileArgs& a, cudaStream_t s) {
     constexpr int TX = Shape<L>::TX, TY = Shape<L>::TY;
     const int tiles = (int)(((h.desc.Nx + TX - 1) / TX) * ((p.j_hi - p.j_lo + TY - 1) / TY));
     const bool refract = p.transport == RPL_TRANSPORT_REFRACTION;
     const int src = p.learned ? 2 : ((p.has_wind || p.has_diss) ? 1 : (p.lin_rates ? 3 : 0));
+    if (refract && a.sxy) {
+        if (src == 3) return launch_split<L, 3>(a, s);
+        if (src == 2) return launch_split<L, 2>(a, s);
+        return src ? launch_split<L, 1>(a, s) : launch_split<L, 0>(a, s);
+    }
     if (refract) {
         if (src == 3) return launch_variant<L, true, 3>(a, tiles, s);
         if (src == 2) return launch_variant<L, true, 2>(a, tiles, s);
@@ -524,6 +801,7 @@ TileArgs make_tile_args(const Handle& h, const StageParams& p, const void* Nin, 
     a.lin_rates = static_cast<const float*>(p.lin_rates);
     a.j_lo = (int)p.j_lo;
     a.j_hi = (int)p.j_hi;
+    a.sxy = h.d_sxy;
     return a;
 }
 
