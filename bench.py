@@ -770,7 +770,8 @@ def run_learned(args, rank, world, local_rank):
         _lib.check(lib.rpl_get_action_device(h, _lib.ctypes.c_void_p(state.data_ptr()), _lib.RPL_F32, 0))
         d = rp.diagnostics(m.action)
         res[mode] = dict(ms=ms, clocks=clk.summary(), N=state, Hs=d["Hs"], total=d["total_action"],
-                         fallback=learned.fallback_cells(m) if mode == "learned" else 0)
+                         fallback=learned.fallback_cells(m) if mode == "learned" else 0,
+                         totals=learned.fallback_totals(m) if mode == "learned" else (0, 1))
         m.close()
     a, b = res["learned"], res["plain"]
     dN = float(torch.linalg.vector_norm((a["N"] - b["N"]).double()) / torch.linalg.vector_norm(b["N"].double()))
@@ -814,6 +815,7 @@ def run_learned(args, rank, world, local_rank):
                        "mean_spectrum_relL2_vs_plain": dS,
                        "total_action_rel_diff": abs(a["total"] - b["total"]) / b["total"],
                        "fallback_cells_last_stage": a["fallback"], "cells": P,
+                       "fallback_cell_stage_fraction": a["totals"][0] / max(1, a["totals"][1]),
                        "training_rows": rows, "training_steps": args.train_steps * (2 + args.dagger) // 2,
                        "dagger_rounds": args.dagger, "feature_pad": args.feature_pad, "learned_gate": args.learned_gate, "training_s": t_train,
                        "data_generation_s": t_data, "losses": losses,

@@ -418,6 +418,9 @@ int rpl_set_learned_gate(rpl_handle* h, double max_rate_dt);
 int rpl_learned_outputs(rpl_handle* h, float* Y);
 /* Cells that fell back to the plain sources in the most recent stage. */
 int rpl_learned_fallback_cells(rpl_handle* h, int64_t* count);
+/* Since rpl_set_learned_source: cell-stages that took the plain sources (out of distribution or gated)
+ * and all cell-stages (cells x stages run with the learned source). */
+int rpl_learned_fallback_totals(rpl_handle* h, int64_t* fallback_cell_stages, int64_t* cell_stages);
 
 /* Device bytes held by the handle. */
 int rpl_device_bytes(rpl_handle* h, int64_t* bytes);

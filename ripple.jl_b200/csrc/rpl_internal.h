@@ -141,6 +141,7 @@ struct Handle {
     int64_t lrows = 0;
     bool lclamp = false;           // clamp the network outputs to the output bounds
     double lgate = 0.0;            // > 0: a cell whose network rates have |rate| * dt above it uses the plain sources
+    unsigned long long* d_lcount = nullptr;  // since rpl_set_learned_source: fallback cell-stages, cell-stages
     bool currents_set = false;
     // prescribed currents: the Q grid and the last currents stay on the device so the coupling can be
     // refreshed (rpl_update_currents*) without allocating

@@ -98,6 +98,16 @@ __global__ void gate_kernel(const float* __restrict__ Y, int64_t P, int nb, floa
     if (lane == 0 && lscale * sinhf(big) > limit) atomicOr(flag + c, 2u);
 }
 
+// Cells of this stage that take the plain sources, added to count[0]; count[1] counts the cells.
+__global__ void count_kernel(const unsigned int* __restrict__ flag, int64_t P, unsigned long long* count) {
+    unsigned long long k = 0;
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < P; c += (int64_t)gridDim.x * blockDim.x)
+        k += flag[c] != 0u;
+    for (int o = 16; o > 0; o >>= 1) k += __shfl_xor_sync(0xffffffffu, k, o);
+    if ((threadIdx.x & 31) == 0 && k) atomicAdd(count, k);
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(count + 1, (unsigned long long)P);
+}
+
 RowArgs row_args(const Handle& h, const rpl_mlp_desc& md, const void* Nin) {
     RowArgs a{};
     a.N = (const float*)Nin;
@@ -153,15 +163,18 @@ cudaError_t launch_learned_stage_prep(const Handle& h, const void* Nin, double d
                                                               (float)(h.lgate / dt), h.d_lflag);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
+    count_kernel<<<148, 256, 0, s>>>(h.d_lflag, h.cells, h.d_lcount);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
     // the stress cap of the plain sources, for the cells that take them
     if (h.src.stress_cap) e = launch_stress_factor(h, Nin, s, h.d_lflag);
     return e;
 }
 
 void free_learned(Handle* h) {
-    void* ps[] = {h->d_lx, h->d_le, h->d_lr, h->d_lflag, h->d_lbounds};
+    void* ps[] = {h->d_lx, h->d_le, h->d_lr, h->d_lflag, h->d_lbounds, h->d_lcount};
     for (void* p : ps)
         if (p) cudaFree(p);
+    h->d_lcount = nullptr;
     h->d_lx = nullptr;
     h->d_le = h->d_lr = h->d_lbounds = nullptr;
     h->d_lflag = nullptr;
@@ -226,7 +239,7 @@ int rpl_set_learned_source(rpl_handle* hh, rpl_mlp* m, const float* lo, const fl
     if ((e = al(&h->d_lx, rows * nb * 2)) != cudaSuccess || (e = al(&h->d_le, rows * 16)) != cudaSuccess ||
         (e = al(&h->d_lr, rows * nb * 4)) != cudaSuccess ||
         (e = al(&h->d_lflag, h->cells * sizeof(unsigned int))) != cudaSuccess ||
-        (e = al(&h->d_lbounds, nbound * 4)) != cudaSuccess) {
+        (e = al(&h->d_lbounds, nbound * 4)) != cudaSuccess || (e = al(&h->d_lcount, 16)) != cudaSuccess) {
         rpl::free_learned(h);
         return rpl::lfail(e == cudaErrorMemoryAllocation ? RPL_ERR_OOM : RPL_ERR_CUDA, "learned-source buffers");
     }
@@ -240,6 +253,7 @@ int rpl_set_learned_source(rpl_handle* hh, rpl_mlp* m, const float* lo, const fl
     if ((e = cudaMemsetAsync(h->d_lx, 0, rows * nb * 2, h->stream)) != cudaSuccess ||
         (e = cudaMemsetAsync(h->d_le, 0, rows * 16, h->stream)) != cudaSuccess ||
         (e = cudaMemsetAsync(h->d_lflag, 0, h->cells * sizeof(unsigned int), h->stream)) != cudaSuccess ||
+        (e = cudaMemsetAsync(h->d_lcount, 0, 16, h->stream)) != cudaSuccess ||
         (e = cudaMemcpyAsync(h->d_lbounds, b.data(), b.size() * 4, cudaMemcpyHostToDevice, h->stream)) != cudaSuccess ||
         (e = cudaStreamSynchronize(h->stream)) != cudaSuccess) {
         rpl::free_learned(h);
@@ -268,6 +282,21 @@ int rpl_learned_outputs(rpl_handle* hh, float* Y) {
     cudaError_t e = cudaMemcpyAsync(Y, h->d_lr, bytes, cudaMemcpyDeviceToHost, h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) return rpl::lfail(RPL_ERR_CUDA, "rpl_learned_outputs");
+    return RPL_OK;
+}
+
+int rpl_learned_fallback_totals(rpl_handle* hh, int64_t* fallback_cell_stages, int64_t* cell_stages) {
+    if (!hh || !fallback_cell_stages || !cell_stages) return rpl::lfail(RPL_ERR_ARGUMENT, "null argument");
+    Handle* h = reinterpret_cast<Handle*>(hh);
+    *fallback_cell_stages = *cell_stages = 0;
+    if (!h->learned) return RPL_OK;
+    cudaSetDevice(h->device);
+    unsigned long long v[2] = {0, 0};
+    cudaError_t e = cudaMemcpyAsync(v, h->d_lcount, 16, cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return rpl::lfail(RPL_ERR_CUDA, "rpl_learned_fallback_totals");
+    *fallback_cell_stages = (int64_t)v[0];
+    *cell_stages = (int64_t)v[1];
     return RPL_OK;
 }
 

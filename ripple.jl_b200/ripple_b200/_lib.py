@@ -151,6 +151,7 @@ _SIGNATURES = {
     "rpl_gemm_bf16_bounded": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, _i32, _i32, _i32,
                                              ctypes.c_uint32, ctypes.c_void_p]),
     "rpl_set_learned_gate": (ctypes.c_int, [ctypes.c_void_p, _d]),
+    "rpl_learned_fallback_totals": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
     "rpl_learned_sample": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                           ctypes.c_void_p]),
     "rpl_set_learned_source": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,

@@ -160,6 +160,13 @@ def fallback_cells(model):
     return n.value
 
 
+def fallback_totals(model):
+    """(cell-stages that took the plain sources, all cell-stages) since the learned source was set."""
+    f, t = ctypes.c_int64(), ctypes.c_int64()
+    check(model._lib.rpl_learned_fallback_totals(model.handle, ctypes.byref(f), ctypes.byref(t)))
+    return f.value, t.value
+
+
 def input_bounds(X, E, margin=0.05, feature_pad=0.25, extra_pad=0.02):
     """Per-input [lo, hi] of a training set (X bf16 rows, E rows), widened by `margin` of each input's range
     plus an absolute pad: `feature_pad` for the log-action features (0.25 = a factor e^(0.25 feature_scale)

@@ -256,9 +256,11 @@ def test_learned_trust_gate(torch):
         rp.time_step(m, w.dt, 3)
         learned.use_learned_source(m, net, lo, hi, gate=gate)
         rp.time_step(m, w.dt, 2)
-        res[name] = (m.action.interior().copy(), learned.fallback_cells(m))
+        res[name] = (m.action.interior().copy(), learned.fallback_cells(m), learned.fallback_totals(m))
         m.close()
+    P = w.grid.Nx * w.grid.Ny
     assert np.array_equal(res["none"][0], res["huge"][0]) and res["none"][1] == res["huge"][1] == 0
-    assert res["small"][1] > 0
+    assert res["none"][2] == (0, 6 * P)                       # 2 steps x 3 stages, no cell fell back
+    assert res["small"][1] > 0 and 0 < res["small"][2][0] <= 6 * P
     assert not np.array_equal(res["small"][0], res["none"][0])
     net.close()
