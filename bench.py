@@ -97,6 +97,9 @@ CONFIG_STEPS = {"seamount": 200, "hurricane": 1000, "selfcoupled": 200}   # RK3 
 WORKLOAD_NAMES = {"seamount": "seamount_eddies", "hurricane": "hurricane_swell", "ensemble": "ensemble_members",
                   "learned": "hurricane_swell (learned source)", "selfcoupled": "self_coupled_swell"}
 TRAFFIC_SUFFIX = {"seamount": "", "hurricane": "_hurricane", "selfcoupled": "_selfcoupled"}
+# the FP32 stage kernels each workload runs (refraction: two passes per stage; intrinsic: one fused kernel)
+STAGE_KERNELS = {"seamount": "xy_kernel+kp_kernel", "hurricane": "tile_kernel",
+                 "selfcoupled": "xy_kernel+kp_kernel"}
 DATA = {"seamount": "synthetic (seeded seamount depth, eddy currents, JONSWAP-like N0)",
         "hurricane": "synthetic (Holland hurricane on a linear track, uniform N0 = 1e-6)",
         "selfcoupled": "synthetic (Gaussian swell packet, 50 m depth, pseudomomentum self-coupling)"}
@@ -118,10 +121,20 @@ def make_workload(name, n, nsteps, n0_dtype=np.float64):
     return w
 
 
-def launches_per_step(name):
-    """Our kernels per RK3 step: 3 fused stage kernels; the hurricane adds 1 wind + 3 stress-cap kernels;
-    the self-coupled swell adds 2 coupling kernels per stage."""
-    return {"seamount": 3, "selfcoupled": 9}.get(name, 7)
+def launches_per_step(name, precision="fp32"):
+    """Our kernels per RK3 step. A refraction stage is two launches in FP32 (x/y flux pass, then the
+    kappa/phi pass with the stage update) and one fused launch in FP64; the hurricane (intrinsic
+    transport, one fused launch per stage) adds 1 wind + 3 stress-cap kernels; the self-coupled swell
+    adds 2 coupling kernels per stage, and in FP32 the refresh of the velocity planes of the x/y pass."""
+    per_stage = 2 if precision == "fp32" else 1
+    coupling = 3 if precision == "fp32" else 2
+    return {"seamount": 3 * per_stage, "selfcoupled": 3 * (per_stage + coupling)}.get(name, 7)
+
+
+def current_launches(precision):
+    """Kernels of one update of time-varying currents: Q transform, gradients, coefficient records, and
+    in FP32 the velocity planes of the x/y pass."""
+    return 4 if precision == "fp32" else 3
 
 
 def peaks():
@@ -514,7 +527,7 @@ def run_ours(args, rank, world, local_rank):
                           if snap_bufs is not None else {})},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": "tile_kernel" if args.precision == "fp32" else "column_kernel",
+                         "kernel": STAGE_KERNELS[args.workload] if args.precision == "fp32" else "column_kernel",
                          "launch_ms": launch_ms, "algorithmic_bytes_per_launch": bytes_per_launch,
                          "launch_interval": "one RK3 stage" + {"seamount": "",
                                                                "selfcoupled": " incl. its coupling refresh"}.get(
@@ -523,7 +536,7 @@ def run_ours(args, rank, world, local_rank):
             **({"rel_l2_vs_fp64": acc["rel_l2_vs_fp64"], "action_drift": acc["action_drift"],
                 "fp64_ms_per_step": acc["fp64_ms_per_step"],
                 "speedup_vs_fp64": acc["fp64_ms_per_step"] / (ms / args.steps), "accuracy": acc} if acc else {}),
-            "gpu_launches": (launches_per_step(args.workload) + (3 if cur else 0) + (2 if snap_bufs else 0)
+            "gpu_launches": (launches_per_step(args.workload, args.precision) + (current_launches(args.precision) if cur else 0) + (2 if snap_bufs else 0)
                              + (1 if args.smoothing else 0)) * args.steps
                             + (args.steps // args.output_every if snap_bufs else 0),
             "clocks": clocks,
@@ -920,7 +933,9 @@ def run_decomposed(args, rank, world, local_rank):
                                                               "every stage",
                        "rows_per_rank": dm.slab.ny},
             "roofline": None, "cpu_baseline": None, "e2e": None,
-            "gpu_launches": launches_per_step(args.workload) * args.steps, "clocks": clk.summary(),
+            # every stage runs as three row ranges (interior, then the two boundary ranges after the exchange)
+            "gpu_launches": 3 * launches_per_step(args.workload, args.precision) * args.steps,
+            "clocks": clk.summary(),
         }
         print(json.dumps(line), flush=True)
     dm.model.close()

@@ -77,7 +77,8 @@ void free_all(Handle* h) {
     rpl::free_currents(h);
     void* ptrs[] = {h->N, h->A, h->B, h->d_kappa, h->d_phi, h->d_cos, h->d_sin, h->d_weights, h->d_cgx,
                     h->d_cgy, h->d_cgmag, h->d_depth, h->d_coupling, h->d_wind, h->d_diag, h->d_err,
-                    h->d_coef, h->d_tab32, h->d_cell32, h->d_bin32, h->d_U, h->d_spacing, h->d_sxy};
+                    h->d_coef, h->d_tab32, h->d_cell32, h->d_bin32, h->d_U, h->d_spacing, h->d_sxy,
+                    h->d_vel32, h->d_rmax};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->h_err) cudaFreeHost(h->h_err);
@@ -259,7 +260,7 @@ int rpl_create(const rpl_desc* d, rpl_handle** out) {
     const int64_t c3 = d->Nx * d->Ny * d->Nk, P = d->Nx * d->Ny, nb = d->Nk * d->Np;
     int64_t need = 3 * units * (int64_t)elem + 16 * c3 * 8 + (d->depth_kind == RPL_DEPTH_FIELD ? (c3 + P) * 8 : 0) +
                    (4 * P + 2 * (d->Nx + d->Ny)) * 8 + 6 * P * 8 + 8 * nb * 8 +
-                   (d->precision == RPL_FP32 && d->transport == RPL_TRANSPORT_REFRACTION ? units * 4 : 0);
+                   (d->precision == RPL_FP32 && d->transport == RPL_TRANSPORT_REFRACTION ? units * 4 + 3 * c3 * 4 : 0);
     if (d->memory_limit_bytes > 0 && need > d->memory_limit_bytes)
         return fail(RPL_ERR_OOM, "model needs " + std::to_string(need) + " device bytes, above the memory limit of " +
                                      std::to_string(d->memory_limit_bytes));
@@ -270,6 +271,8 @@ int rpl_create(const rpl_desc* d, rpl_handle** out) {
     {
         const char* env = std::getenv("RPL_FORCE_COLUMN_KERNEL");
         h->force_column_kernel = env && env[0] == '1';
+        const char* pa = std::getenv("RPL_PASS_A");
+        h->pass_a_tiles = pa && std::string(pa) == "tiles";
     }
     h->device = d->device;
     h->precision = d->precision;
@@ -392,6 +395,11 @@ int rpl_create(const rpl_desc* d, rpl_handle** out) {
     TRY(dalloc(h, &h->d_bin32, 8 * d->Nk));
     if (d->transport == RPL_TRANSPORT_REFRACTION && rpl::tile32_supported(*h) && !h->force_column_kernel)
         TRY(dalloc(h, &h->d_sxy, units));  // the two-pass refraction stage of FP32 models
+    if (h->d_sxy && rpl::xyw_supported(*h) && !h->pass_a_tiles) {   // its y-walk pass A: FP32 velocity planes, upwind ratios
+        TRY(dalloc(h, &h->d_vel32, 3 * c3));
+        h->vel_regions = rpl::xyw_regions(*h);
+        TRY(dalloc(h, &h->d_rmax, 2 * h->vel_regions * d->Nk));
+    }
     TRY(rpl::launch_coef(*h, s));
     {
         std::vector<float> tab32(6 * d->Np + 3 * nb);

@@ -84,6 +84,12 @@ struct TileArgs {
     const float* lin_rates;  // SourceTermSet rates per cell-bin (state layout) or null
     int j_lo, j_hi;          // rows the stage updates
     float* sxy;              // two-pass refraction stage: x+y flux sums per cell-bin (state layout), or null
+    // y-walk pass A (rpl_xyw.cu), or null: FP32 planes of U_x, U_y and the c_g magnitude per (i,j,m),
+    // and the per-region upwind ratios
+    const float* ux32;
+    const float* uy32;
+    const float* cgc32;
+    const unsigned int* rmax;
 };
 
 // Tile shapes (kappa-pair lanes per cell L, tile TX x TY) compiled into the ensemble kernel; every
@@ -131,6 +137,9 @@ struct Handle {
     float* d_cell32 = nullptr;     // (Nx*Ny) x 8 floats of per-cell wind constants
     float* d_bin32 = nullptr;      // Nk x 8 floats of per-kappa source constants
     float* d_sxy = nullptr;        // FP32 refraction models: x+y flux sums between the two stage passes
+    float* d_vel32 = nullptr;      // y-walk pass A: FP32 planes U_x, U_y, c_g per (i,j,m) (3 x Nx*Ny*Nk)
+    unsigned int* d_rmax = nullptr;  // y-walk pass A: per region, axis and bin the upwind ratio maxima
+    int64_t vel_regions = 0;
     // learned source (rpl_learned.cu)
     rpl_mlp* learned = nullptr;
     void* d_lx = nullptr;          // (rows x nbins) BF16 features, rows = cells rounded up to 128
@@ -193,6 +202,7 @@ struct Handle {
     unsigned int* d_err = nullptr;
     unsigned int* h_err = nullptr;  // pinned
     bool force_column_kernel = false;  // RPL_FORCE_COLUMN_KERNEL=1 selects the generic FP32 column kernel
+    bool pass_a_tiles = false;         // RPL_PASS_A=tiles: pass A of FP32 refraction from staged tiles
     double time = 0.0;
     int64_t iteration = 0;
     int64_t bytes = 0;
@@ -253,6 +263,15 @@ cudaError_t launch_coef(const Handle& h, cudaStream_t s);
 cudaError_t launch_coef_from_U(const Handle& h, cudaStream_t s);
 // d_U -> the caller-order coupling arrays 0-3 of d_coupling, then their gradients (arrays 4-7).
 cudaError_t launch_export_U(const Handle& h, cudaStream_t s);
+
+// ---- y-walk pass A of the FP32 refraction stage (rpl_xyw.cu) ----
+bool xyw_supported(const Handle& h);              // 32-bit offsets within a direction slice
+int xyw_lanes(int64_t Nk);                        // lanes per cell (four kappa bins each)
+int64_t xyw_regions(const Handle& h);             // regions of the upwind ratio table
+// FP32 velocity planes and upwind ratios from d_coef (after every coefficient refresh; no-op without
+// d_vel32).
+cudaError_t launch_vel32(const Handle& h, cudaStream_t s);
+cudaError_t launch_xyw(const TileArgs& a, cudaStream_t s);   // writes a.sxy for rows [j_lo, j_hi)
 
 // ---- FP32 tiled stage kernel (rpl_tile32.cu) ----
 bool tile32_supported(const Handle& h);

@@ -164,7 +164,8 @@ cudaError_t launch_coef(const Handle& h, cudaStream_t s) {
     const int64_t c3 = d.Nx * d.Ny * d.Nk;
     coef_kernel<<<(unsigned)((c3 + 255) / 256), 256, 0, s>>>(d.Nx, d.Ny, d.Nk, h.currents_set ? h.d_coupling : nullptr,
                                                              h.d_cgmag, h.d_kappa, h.d_coef);
-    return cudaGetLastError();
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? launch_vel32(h, s) : e;
 }
 
 cudaError_t launch_coef_from_U(const Handle& h, cudaStream_t s) {
@@ -172,7 +173,8 @@ cudaError_t launch_coef_from_U(const Handle& h, cudaStream_t s) {
     const int64_t c3 = d.Nx * d.Ny * d.Nk;
     coef_from_U_kernel<<<(unsigned)((c3 + COEF_THREADS - 1) / COEF_THREADS), COEF_THREADS, 0, s>>>(
         d.Nx, d.Ny, (int)d.Nk, h.d_U, 1.0 / d.dx, 1.0 / d.dy, h.d_coef);
-    return cudaGetLastError();
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? launch_vel32(h, s) : e;
 }
 
 cudaError_t launch_export_U(const Handle& h, cudaStream_t s) {

@@ -249,6 +249,41 @@ def test_fp32_kernels_edge_sizes(oracle_mod, monkeypatch, shape, column_kernel):
     assert rel_l2(Ng, No) <= FP32_TOL
 
 
+def pass_a_workload(shape, current, seed, depth_field=False):
+    Nx, Ny, Nk, Np = shape
+    rng = np.random.default_rng(seed)
+    if depth_field:
+        w = workloads.seamount_eddies(N=Nx, Nz=4, Nk=Nk, Np=Np, nsteps=3)
+        return w
+    g = rp.RectilinearGrid(size=(Nx, Ny, 4), x=(0.0, Nx * 2.0), y=(0.0, Ny * 2.0), z=(-3.0, 0.0))
+    sg = rp.PolarWaveVectorGrid(κ=np.linspace(0.3, 0.9, Nk), φ=np.arange(Np) * 2 * math.pi / Np)
+    u = np.asfortranarray(rng.uniform(-current, current, (Nx, Ny, 4)))
+    v = np.asfortranarray(rng.uniform(-current, current, (Nx, Ny, 4)))
+    N0 = np.asfortranarray(rng.uniform(0.5, 1.0, shape))
+    return workloads.Workload("pass_a", g, sg, 2.0, N0, 0.05, 3, velocities={"u": u, "v": v})
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape,current,depth_field", [
+    ((3, 5, 4, 3), 0.3, False), ((37, 29, 8, 7), 0.3, False), ((20, 9, 24, 12), 0.3, False),
+    ((17, 11, 32, 36), 0.3, False), ((33, 300, 16, 8), 0.05, False), ((70, 140, 32, 12), 3.0, False),
+    ((40, 40, 32, 24), 0.0, False), ((48, 48, 32, 36), 0.0, True)])
+def test_fp32_pass_a_forms_agree_bitwise(monkeypatch, shape, current, depth_field):
+    """The y-walk pass A (one reconstruction per face, uniform-sign CTAs without selects) and the tile
+    form give the same FP32 state bit for bit after three SSP-RK3 steps: partial x tiles, several
+    128-row segments, weak, strong and no currents (uniform and mixed upwind CTAs), c_g per cell."""
+    w = pass_a_workload(shape, current, 11 + sum(shape), depth_field)
+    out = {}
+    for form in ("", "tiles"):
+        monkeypatch.setenv("RPL_PASS_A", form)
+        m = w.model("fp32")
+        rp.time_step(m, w.dt, 3)
+        out[form] = m.action.interior()
+        m.close()
+    assert np.all(np.isfinite(out[""])) and np.max(np.abs(out[""])) > 0
+    assert np.array_equal(out[""], out["tiles"])
+
+
 @pytest.mark.parametrize("column_kernel", ["0", "1"])
 def test_fp32_kernels_intrinsic_and_depth_field(oracle_mod, monkeypatch, column_kernel):
     monkeypatch.setenv("RPL_FORCE_COLUMN_KERNEL", column_kernel)
