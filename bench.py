@@ -58,7 +58,7 @@ def parse():
                     help="absolute widening of the per-bin log-action input bounds beyond the training rows, in "
                          "feature units (x 4 in log N); a cell outside the bounds uses the plain sources "
                          "(--workload learned)")
-    ap.add_argument("--learned-gate", type=float, default=0.0,
+    ap.add_argument("--learned-gate", type=float, default=0.02,
                     help="trust gate of the learned source: cells whose network rates exceed this fraction of "
                          "the action per step use the plain sources (0: off; --workload learned)")
     ap.add_argument("--calm-fraction", type=float, default=0.05,
