@@ -273,6 +273,8 @@ int rpl_create(const rpl_desc* d, rpl_handle** out) {
         h->force_column_kernel = env && env[0] == '1';
         const char* pa = std::getenv("RPL_PASS_A");
         h->pass_a_tiles = pa && std::string(pa) == "tiles";
+        const char* pb = std::getenv("RPL_PASS_B");
+        h->pass_b_pairs = pb && std::string(pb) == "pairs";
     }
     h->device = d->device;
     h->precision = d->precision;

@@ -80,7 +80,7 @@ struct TileArgs {
     float lscale;
     const float* lrate;
     const unsigned int* lflag;
-    int learned, pad1;
+    int learned, pass_b_quads;   // pass_b_quads: pass B of SRC 0/3 stages with four kappa bins per lane
     const float* lin_rates;  // SourceTermSet rates per cell-bin (state layout) or null
     int j_lo, j_hi;          // rows the stage updates
     float* sxy;              // two-pass refraction stage: x+y flux sums per cell-bin (state layout), or null
@@ -203,6 +203,7 @@ struct Handle {
     unsigned int* h_err = nullptr;  // pinned
     bool force_column_kernel = false;  // RPL_FORCE_COLUMN_KERNEL=1 selects the generic FP32 column kernel
     bool pass_a_tiles = false;         // RPL_PASS_A=tiles: pass A of FP32 refraction from staged tiles
+    bool pass_b_pairs = false;         // RPL_PASS_B=pairs: pass B with two kappa bins per lane throughout
     double time = 0.0;
     int64_t iteration = 0;
     int64_t bytes = 0;

@@ -276,8 +276,8 @@ __device__ __forceinline__ void tile_body(const TileArgs& p, int tile, float* sm
                                          make_float2(pa ? k1 : km2, 0.f));
                 Flo = hlo ? t.x : (pa ? km1 : k0);
             }
-            const float fk0 = ((m0 == Nk - 1) ? 0.f : ck.x * Fab.x) - ((m0 == 0) ? 0.f : ck.x * Flo);
-            const float fk1 = ((m0 + 1 == Nk - 1) ? 0.f : ck.y * Fab.y) - ck.y * Fam1;
+            const float fk0 = kflux(m0 == Nk - 1, m0 == 0, ck.x, Fab.x, Flo);
+            const float fk1 = kflux(m0 + 1 == Nk - 1, false, ck.y, Fab.y, Fam1);
             const float2 fk = mul2(make_float2(fk0, fk1), f2(dk_inv));
             // phi: window
             const bool qx = cp.x >= 0.f, qy = cp.y >= 0.f;
@@ -539,8 +539,8 @@ __global__ void __launch_bounds__(CPB * L, MINB) kp_kernel(const TileArgs p) {
                                      make_float2(pa ? k1 : km2, 0.f));
             Flo = hlo ? t.x : (pa ? km1 : k0);
         }
-        const float fk0 = ((m0 == Nk - 1) ? 0.f : ck.x * Fab.x) - ((m0 == 0) ? 0.f : ck.x * Flo);
-        const float fk1 = ((m0 + 1 == Nk - 1) ? 0.f : ck.y * Fab.y) - ck.y * Fam1;
+        const float fk0 = kflux(m0 == Nk - 1, m0 == 0, ck.x, Fab.x, Flo);
+        const float fk1 = kflux(m0 + 1 == Nk - 1, false, ck.y, Fab.y, Fam1);
         const float2 fk = mul2(make_float2(fk0, fk1), f2(dk_inv));
         const bool qx = cp.x >= 0.f, qy = cp.y >= 0.f;
         float2 Fpp;
@@ -587,6 +587,176 @@ __global__ void __launch_bounds__(CPB * L, MINB) kp_kernel(const TileArgs p) {
             *reinterpret_cast<float2*>(Nout + slice * n + home) = out;
         }
         w0 = w1; w1 = w2; w2 = w3; w3 = w4; w4 = w5; w5 = w6; w6 = nxt;
+    }
+}
+
+// Pass B with four kappa bins per lane (two packed pairs), for stages without the bundle or learned
+// sources (SRC 0 and 3): the pair kernel's arithmetic element for element, with per-lane overhead
+// (shuffles, window bookkeeping, addressing) shared by four bins. The kappa stencil m0-3 .. m0+6 comes
+// from the lanes below and above (three shuffles each, the reference's clamped indices: Nk % 4 == 0, so
+// only the lowest and the highest live lane clamp).
+template <int L, int CPB, int MINB, int SRC>
+__global__ void __launch_bounds__(CPB * L, MINB) kq_kernel(const TileArgs p) {
+    static_assert(SRC == 0 || SRC == 3, "bundle and learned sources use the pair kernel");
+    const float* __restrict__ S = p.sxy;
+    const float* __restrict__ Nin = p.Nin;
+    const float* N0 = p.N0;
+    float* Nout = p.Nout;
+    const int Nx = p.Nx, Ny = p.Ny, Nk = p.Nk, Np = p.Np;
+    const int64_t slice = (int64_t)Nx * Ny * Nk;
+    const int64_t P = (int64_t)Nx * (p.j_hi - p.j_lo);
+    const int tid = threadIdx.x, l = tid % L;
+    const int64_t cidx = (int64_t)blockIdx.x * CPB + tid / L;
+    const bool live_cell = cidx < P;
+    const int64_t cc = (live_cell ? cidx : P - 1) + (int64_t)Nx * p.j_lo;
+    const int m0 = 4 * l;
+    const bool live = live_cell && m0 < Nk;
+    const int mc = m0 < Nk ? m0 : Nk - 4;
+    const int64_t home = cc * Nk + mc;
+    const double* r0 = p.coef + 8 * home;
+    auto cq = [&](int f) {
+        return Q{make_float2((float)r0[f], (float)r0[8 + f]), make_float2((float)r0[16 + f], (float)r0[24 + f])};
+    };
+    const Q kap = cq(7), Uxx = cq(2), Uxy = cq(3), Uyx = cq(4), Uyy = cq(5);
+    const float* own = Nin + home;
+    auto wr = [&](int n) { return n < 0 ? n + Np : (n >= Np ? n - Np : n); };
+    Q w0 = ldq(own + slice * wr(-3)), w1 = ldq(own + slice * wr(-2)), w2 = ldq(own + slice * wr(-1));
+    Q w3 = ldq(own), w4 = ldq(own + slice * wr(1)), w5 = ldq(own + slice * wr(2)), w6 = ldq(own + slice * wr(3));
+    const float dk_inv = p.dk_inv, dp_inv = p.dp_inv, dt = p.dt, ca = p.a, cb = p.b;
+    auto full = [&](int q) { return q - 2 >= 0 && q + 3 <= Nk - 1; };   // face q|q+1 has its 5-point stencil
+    const bool hlo = full(m0 - 1), ha = full(m0), hb = full(m0 + 1), hc = full(m0 + 2), hd = full(m0 + 3);
+    const bool up = m0 + 4 <= Nk - 1;   // bins above the quad exist (else clamped to the last bin)
+    Q prevF = qz();
+    bool pvx = false, pvy = false, pvz = false, pvw = false, have = false;
+    for (int n = 0; n < Np; ++n) {
+        const int64_t off = slice * n + home;
+        const Q nxt = ldq(own + slice * ((n + 4) % Np));
+        const Q n0v = (p.stage == 1 || !live) ? qz() : ldq(N0 + off);
+        const Q sxy = ldq(S + off);
+        const Q c = w3;
+        const float4 tg = __ldg(p.trig32 + n);
+        auto ckf = [&](float2 kp_, float2 xx, float2 xy, float2 yx, float2 yy) {
+            return mul2(mul2(f2(-1.f), kp_),
+                        add2(add2(mul2(f2(tg.x), xx), mul2(f2(tg.y), add2(yx, xy))), mul2(f2(tg.z), yy)));
+        };
+        auto cpf = [&](float2 xx, float2 xy, float2 yx, float2 yy) {
+            return sub2(add2(mul2(f2(tg.y), sub2(xx, yy)), mul2(f2(tg.z), yx)), mul2(f2(tg.x), xy));
+        };
+        const Q ck = {ckf(kap.a, Uxx.a, Uxy.a, Uyx.a, Uyy.a), ckf(kap.b, Uxx.b, Uxy.b, Uyx.b, Uyy.b)};
+        const Q cp = {cpf(Uxx.a, Uxy.a, Uyx.a, Uyy.a), cpf(Uxx.b, Uxy.b, Uyx.b, Uyy.b)};
+        const float k0 = c.a.x, k1 = c.a.y, k2 = c.b.x, k3 = c.b.y;
+        const float s_m3 = __shfl_sync(FULL, k1, l - 1, L), s_m2 = __shfl_sync(FULL, k2, l - 1, L);
+        const float s_m1 = __shfl_sync(FULL, k3, l - 1, L);
+        const float s_p4 = __shfl_sync(FULL, k0, l + 1, L), s_p5 = __shfl_sync(FULL, k1, l + 1, L);
+        const float s_p6 = __shfl_sync(FULL, k2, l + 1, L);
+        const float km3 = l >= 1 ? s_m3 : k0, km2 = l >= 1 ? s_m2 : k0, km1 = l >= 1 ? s_m1 : k0;
+        const float kp4 = up ? s_p4 : k3, kp5 = up ? s_p5 : k3, kp6 = up ? s_p6 : k3;
+        // upper faces a..d of bins m0..m0+3, each upwinded by its own bin
+        const bool pa = ck.a.x >= 0.f, pb = ck.a.y >= 0.f, pc = ck.b.x >= 0.f, pd = ck.b.y >= 0.f;
+        float2 Fab, Fcd;
+        if (__all_sync(FULL, pa && pb && pc && pd)) {
+            Fab = weno5_2(make_float2(km2, km1), make_float2(km1, k0), make_float2(k0, k1), make_float2(k1, k2),
+                          make_float2(k2, k3));
+            Fcd = weno5_2(make_float2(k0, k1), make_float2(k1, k2), make_float2(k2, k3), make_float2(k3, kp4),
+                          make_float2(kp4, kp5));
+        } else if (__all_sync(FULL, !pa && !pb && !pc && !pd)) {
+            Fab = weno5_2(make_float2(k3, kp4), make_float2(k2, k3), make_float2(k1, k2), make_float2(k0, k1),
+                          make_float2(km1, k0));
+            Fcd = weno5_2(make_float2(kp5, kp6), make_float2(kp4, kp5), make_float2(k3, kp4), make_float2(k2, k3),
+                          make_float2(k1, k2));
+        } else {
+            Fab = weno5_2(make_float2(pa ? km2 : k3, pb ? km1 : kp4), make_float2(pa ? km1 : k2, pb ? k0 : k3),
+                          make_float2(pa ? k0 : k1, pb ? k1 : k2), make_float2(pa ? k1 : k0, pb ? k2 : k1),
+                          make_float2(pa ? k2 : km1, pb ? k3 : k0));
+            Fcd = weno5_2(make_float2(pc ? k0 : kp5, pd ? k1 : kp6), make_float2(pc ? k1 : kp4, pd ? k2 : kp5),
+                          make_float2(pc ? k2 : k3, pd ? k3 : kp4), make_float2(pc ? k3 : k2, pd ? kp4 : k3),
+                          make_float2(pc ? kp4 : k1, pd ? kp5 : k2));
+        }
+        const float Fa = ha ? Fab.x : (pa ? k0 : k1), Fb = hb ? Fab.y : (pb ? k1 : k2);
+        const float Fc = hc ? Fcd.x : (pc ? k2 : k3), Fd = hd ? Fcd.y : (pd ? k3 : kp4);
+        // lower faces: of m0 the lane below's face d (upwinded by bin m0-1), of m0+1..m0+3 the faces
+        // a..c; recomputed in the bin's own orientation where the two bins' signs differ
+        const float upF = __shfl_up_sync(FULL, Fd, 1, L);
+        const bool upP = __shfl_up_sync(FULL, (int)pd, 1, L) != 0;
+        const bool mA0 = m0 >= 1 && upP != pa, mA1 = pa != pb, mB0 = pb != pc, mB1 = pc != pd;
+        float loA0 = upF, loA1 = Fa, loB0 = Fb, loB1 = Fc;
+        if (mA0 || mA1) {
+            const float2 t = weno5_2(make_float2(pa ? km3 : k2, pb ? km2 : k3), make_float2(pa ? km2 : k1, pb ? km1 : k2),
+                                     make_float2(pa ? km1 : k0, pb ? k0 : k1), make_float2(pa ? k0 : km1, pb ? k1 : k0),
+                                     make_float2(pa ? k1 : km2, pb ? k2 : km1));
+            if (mA0) loA0 = hlo ? t.x : (pa ? km1 : k0);
+            if (mA1) loA1 = ha ? t.y : (pb ? k0 : k1);
+        }
+        if (mB0 || mB1) {
+            const float2 t = weno5_2(make_float2(pc ? km1 : kp4, pd ? k0 : kp5), make_float2(pc ? k0 : k3, pd ? k1 : kp4),
+                                     make_float2(pc ? k1 : k2, pd ? k2 : k3), make_float2(pc ? k2 : k1, pd ? k3 : k2),
+                                     make_float2(pc ? k3 : k0, pd ? kp4 : k1));
+            if (mB0) loB0 = hb ? t.x : (pc ? k1 : k2);
+            if (mB1) loB1 = hc ? t.y : (pd ? k2 : k3);
+        }
+        const Q fk = {mul2(make_float2(kflux(m0 == Nk - 1, m0 == 0, ck.a.x, Fa, loA0),
+                                       kflux(m0 + 1 == Nk - 1, false, ck.a.y, Fb, loA1)), f2(dk_inv)),
+                      mul2(make_float2(kflux(m0 + 2 == Nk - 1, false, ck.b.x, Fc, loB0),
+                                       kflux(m0 + 3 == Nk - 1, false, ck.b.y, Fd, loB1)), f2(dk_inv))};
+        // phi faces: the upper from the window, the lower carried from the previous step unless the sign changed
+        const bool qx = cp.a.x >= 0.f, qy = cp.a.y >= 0.f, qz_ = cp.b.x >= 0.f, qw = cp.b.y >= 0.f;
+        Q Fpp;
+        if (__all_sync(FULL, qx && qy && qz_ && qw)) Fpp = qweno(w1, w2, w3, w4, w5);
+        else if (__all_sync(FULL, !qx && !qy && !qz_ && !qw)) Fpp = qweno(w6, w5, w4, w3, w2);
+        else
+            Fpp = {weno5_2(sel2(qx, qy, w1.a, w6.a), sel2(qx, qy, w2.a, w5.a), sel2(qx, qy, w3.a, w4.a),
+                           sel2(qx, qy, w4.a, w3.a), sel2(qx, qy, w5.a, w2.a)),
+                   weno5_2(sel2(qz_, qw, w1.b, w6.b), sel2(qz_, qw, w2.b, w5.b), sel2(qz_, qw, w3.b, w4.b),
+                           sel2(qz_, qw, w4.b, w3.b), sel2(qz_, qw, w5.b, w2.b))};
+        Q Fpm = prevF;
+        if (!have || pvx != qx || pvy != qy) {
+            const float2 t = weno5_2(sel2(qx, qy, w0.a, w5.a), sel2(qx, qy, w1.a, w4.a), sel2(qx, qy, w2.a, w3.a),
+                                     sel2(qx, qy, w3.a, w2.a), sel2(qx, qy, w4.a, w1.a));
+            if (!have || pvx != qx) Fpm.a.x = t.x;
+            if (!have || pvy != qy) Fpm.a.y = t.y;
+        }
+        if (!have || pvz != qz_ || pvw != qw) {
+            const float2 t = weno5_2(sel2(qz_, qw, w0.b, w5.b), sel2(qz_, qw, w1.b, w4.b), sel2(qz_, qw, w2.b, w3.b),
+                                     sel2(qz_, qw, w3.b, w2.b), sel2(qz_, qw, w4.b, w1.b));
+            if (!have || pvz != qz_) Fpm.b.x = t.x;
+            if (!have || pvw != qw) Fpm.b.y = t.y;
+        }
+        prevF = Fpp;
+        pvx = qx;
+        pvy = qy;
+        pvz = qz_;
+        pvw = qw;
+        have = true;
+        const Q fp = {mul2(mul2(cp.a, sub2(Fpp.a, Fpm.a)), f2(dp_inv)), mul2(mul2(cp.b, sub2(Fpp.b, Fpm.b)), f2(dp_inv))};
+        Q G = {mul2(f2(-1.f), add2(add2(sxy.a, fk.a), fp.a)), mul2(f2(-1.f), add2(add2(sxy.b, fk.b), fp.b))};
+        if constexpr (SRC == 3) {   // SourceTermSet rates of this stage, state layout
+            const Q r = ldq(p.lin_rates + off);
+            G = {fma2(r.a, c.a, G.a), fma2(r.b, c.b, G.b)};
+        }
+        auto upd = [&](float2 g, float2 cv, float2 nv) {
+            float2 st = fma2(f2(dt), g, cv);
+            st.x = relu(st.x);
+            st.y = relu(st.y);
+            float2 out = st;
+            if (p.stage != 1) {
+                out = fma2(f2(ca), nv, mul2(f2(cb), st));
+                out.x = relu(out.x);
+                out.y = relu(out.y);
+            }
+            return out;
+        };
+        const Q out = {upd(G.a, c.a, n0v.a), upd(G.b, c.b, n0v.b)};
+        if (live) {
+            if (!isfinite(out.a.x) || !isfinite(out.a.y) || !isfinite(out.b.x) || !isfinite(out.b.y)) atomicOr(p.err, 1u);
+            stq(Nout + off, out);
+        }
+        w0 = w1;
+        w1 = w2;
+        w2 = w3;
+        w3 = w4;
+        w4 = w5;
+        w5 = w6;
+        w6 = nxt;
     }
 }
 
@@ -671,6 +841,13 @@ cudaError_t launch_split(const TileArgs& a, cudaStream_t s) {
     }
     if (e != cudaSuccess) return e;
     const int64_t cells = (int64_t)a.Nx * (a.j_hi - a.j_lo);
+    if constexpr (SRC == 0 || SRC == 3) {
+        if (a.pass_b_quads) {   // four kappa bins per lane: 128-thread CTAs, four per SM
+            constexpr int L4 = L / 2, QPB = 128 / L4;
+            kq_kernel<L4, QPB, 4, SRC><<<(unsigned)((cells + QPB - 1) / QPB), QPB * L4, 0, s>>>(a);
+            return cudaGetLastError();
+        }
+    }
     // the per-cell source constants of the bundle and the learned source need registers: two CTAs per SM
     constexpr int BMINB = (SRC == 1 || SRC == 2) ? 2 : 3;
     kp_kernel<L, CPB, BMINB, SRC><<<(unsigned)((cells + CPB - 1) / CPB), CPB * L, 0, s>>>(a);
@@ -749,6 +926,7 @@ TileArgs make_tile_args(const Handle& h, const StageParams& p, const void* Nin, 
     a.j_lo = (int)p.j_lo;
     a.j_hi = (int)p.j_hi;
     a.sxy = h.d_sxy;
+    a.pass_b_quads = !h.pass_b_pairs;
     if (h.d_vel32) {
         const int64_t c3 = h.desc.Nx * h.desc.Ny * h.desc.Nk;
         a.ux32 = h.d_vel32;

@@ -71,5 +71,35 @@ __device__ __forceinline__ void weno5_pair2(float2 s0, float2 s1, float2 s2, flo
     hi = weno_face2(d2, d3, d4, d5, D2, D3, D4, A2, A3, A4, s3);
 }
 
+// Four adjacent kappa bins as two packed pairs, and the packed forms used on them.
+struct Q {                            // four adjacent kappa bins
+    float2 a, b;
+};
+__device__ __forceinline__ Q ldq(const float* p) {
+    const float4 v = *reinterpret_cast<const float4*>(p);
+    return {make_float2(v.x, v.y), make_float2(v.z, v.w)};
+}
+__device__ __forceinline__ Q ldgq(const float* p) {
+    const float4 v = __ldg(reinterpret_cast<const float4*>(p));
+    return {make_float2(v.x, v.y), make_float2(v.z, v.w)};
+}
+__device__ __forceinline__ void stq(float* p, Q q) {
+    *reinterpret_cast<float4*>(p) = make_float4(q.a.x, q.a.y, q.b.x, q.b.y);
+}
+__device__ __forceinline__ Q qz() { return {f2(0.f), f2(0.f)}; }
+__device__ __forceinline__ Q qadd(Q x, Q y) { return {add2(x.a, y.a), add2(x.b, y.b)}; }
+__device__ __forceinline__ Q qsub(Q x, Q y) { return {sub2(x.a, y.a), sub2(x.b, y.b)}; }
+__device__ __forceinline__ Q qmul(Q x, Q y) { return {mul2(x.a, y.a), mul2(x.b, y.b)}; }
+__device__ __forceinline__ Q qmuls(Q x, float s) { return {mul2(x.a, f2(s)), mul2(x.b, f2(s))}; }
+__device__ __forceinline__ Q qweno(Q s0, Q s1, Q s2, Q s3, Q s4) {
+    return {weno5_2(s0.a, s1.a, s2.a, s3.a, s4.a), weno5_2(s0.b, s1.b, s2.b, s3.b, s4.b)};
+}
+// kappa flux of one bin, c (F_hi - F_lo) with the face flux of the top bin (top) or of the bottom bin
+// (bottom) taken as zero: both products and the difference rounded separately, so that every kernel
+// gets the same bits however the compiler would otherwise contract them.
+__device__ __forceinline__ float kflux(bool top, bool bottom, float c, float hi, float lo) {
+    return __fsub_rn(top ? 0.f : __fmul_rn(c, hi), bottom ? 0.f : __fmul_rn(c, lo));
+}
+
 }  // namespace w32
 }  // namespace rpl

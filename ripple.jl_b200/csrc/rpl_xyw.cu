@@ -38,28 +38,6 @@ constexpr int XSEG = 128;            // rows per CTA segment (and per region of 
 constexpr int XTHREADS = 256;        // threads per CTA: CX = XTHREADS / L cells
 enum { POS = 0, NEG = 1, MIX = 2 };
 
-struct Q {                            // four adjacent kappa bins
-    float2 a, b;
-};
-__device__ __forceinline__ Q ldq(const float* p) {
-    const float4 v = *reinterpret_cast<const float4*>(p);
-    return {make_float2(v.x, v.y), make_float2(v.z, v.w)};
-}
-__device__ __forceinline__ Q ldgq(const float* p) {
-    const float4 v = __ldg(reinterpret_cast<const float4*>(p));
-    return {make_float2(v.x, v.y), make_float2(v.z, v.w)};
-}
-__device__ __forceinline__ void stq(float* p, Q q) {
-    *reinterpret_cast<float4*>(p) = make_float4(q.a.x, q.a.y, q.b.x, q.b.y);
-}
-__device__ __forceinline__ Q qz() { return {f2(0.f), f2(0.f)}; }
-__device__ __forceinline__ Q qadd(Q x, Q y) { return {add2(x.a, y.a), add2(x.b, y.b)}; }
-__device__ __forceinline__ Q qsub(Q x, Q y) { return {sub2(x.a, y.a), sub2(x.b, y.b)}; }
-__device__ __forceinline__ Q qmul(Q x, Q y) { return {mul2(x.a, y.a), mul2(x.b, y.b)}; }
-__device__ __forceinline__ Q qmuls(Q x, float s) { return {mul2(x.a, f2(s)), mul2(x.b, f2(s))}; }
-__device__ __forceinline__ Q qweno(Q s0, Q s1, Q s2, Q s3, Q s4) {
-    return {weno5_2(s0.a, s1.a, s2.a, s3.a, s4.a), weno5_2(s0.b, s1.b, s2.b, s3.b, s4.b)};
-}
 // bit 0: some element >= 0; bit 1: some element < 0
 __device__ __forceinline__ int code2(float2 u) {
     return ((u.x >= 0.f || u.y >= 0.f) ? 1 : 0) | ((u.x < 0.f || u.y < 0.f) ? 2 : 0);

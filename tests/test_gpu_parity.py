@@ -284,6 +284,31 @@ def test_fp32_pass_a_forms_agree_bitwise(monkeypatch, shape, current, depth_fiel
     assert np.array_equal(out[""], out["tiles"])
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape,current,depth_field,terms", [
+    ((3, 5, 4, 3), 0.3, False, False), ((37, 29, 8, 7), 0.3, False, False), ((20, 9, 24, 12), 0.3, False, True),
+    ((17, 11, 32, 36), 0.3, False, False), ((70, 40, 32, 12), 3.0, False, True), ((48, 48, 32, 36), 0.0, True, False)])
+def test_fp32_pass_b_forms_agree_bitwise(monkeypatch, shape, current, depth_field, terms):
+    """Pass B with four kappa bins per lane (the default for stages without bundle or learned sources)
+    and with two (RPL_PASS_B=pairs) give the same FP32 state bit for bit after three SSP-RK3 steps:
+    few and many kappa bins (the clamped stencil at both ends), mixed kappa and phi upwind signs, c_g per
+    cell, and the SourceTermSet rates."""
+    from ripple_b200.sources import ExponentialWindInput, SourceTermSet, WhitecappingDissipation
+    w = pass_a_workload(shape, current, 5 + sum(shape), depth_field)
+    if terms:
+        w.sources = SourceTermSet(ExponentialWindInput(rate=2e-3, direction=0.6, spreading_power=2),
+                                  WhitecappingDissipation(rate=1e-3, saturation_threshold=0.05))
+    out = {}
+    for form in ("", "pairs"):
+        monkeypatch.setenv("RPL_PASS_B", form)
+        m = w.model("fp32")
+        rp.time_step(m, w.dt, 3)
+        out[form] = m.action.interior()
+        m.close()
+    assert np.all(np.isfinite(out[""])) and np.max(np.abs(out[""])) > 0
+    assert np.array_equal(out[""], out["pairs"])
+
+
 @pytest.mark.parametrize("column_kernel", ["0", "1"])
 def test_fp32_kernels_intrinsic_and_depth_field(oracle_mod, monkeypatch, column_kernel):
     monkeypatch.setenv("RPL_FORCE_COLUMN_KERNEL", column_kernel)
