@@ -230,7 +230,19 @@ int rpl_stage_async(rpl_handle* h, double dt, int32_t stage);
  * rpl_stage_rows_async(h, dt, s, 0, Ny, RPL_STAGE_PREPARE | RPL_STAGE_FINISH). */
 #define RPL_STAGE_PREPARE 1
 #define RPL_STAGE_FINISH 2
+/* With RPL_STAGE_FINISH on stage 3 of a model with SpatialAveraging: finish the stage without the
+ * averaging (stage 3's result stays in the stage buffer A, rpl_rows_get which 1), so that a decomposed
+ * domain can refresh A's halo rows first and then average with rpl_smooth_rows_async. */
+#define RPL_STAGE_DEFER_SMOOTH 4
 int rpl_stage_rows_async(rpl_handle* h, double dt, int32_t stage, int64_t row0, int64_t nrows, int32_t flags);
+/* The SpatialAveraging of a step (propagation_smoothing.jl:60-199, time_step.jl:168) for rows
+ * row0 .. row0+nrows-1 only: reads the stage buffer A (stage 3's result after RPL_STAGE_DEFER_SMOOTH),
+ * writes N. The rows an averaged row reads are up to its corners' reach away (within one row on the
+ * 3 x 3 path); they are the caller's to provide. y_offset: the model's row 0 is row y_offset of a
+ * larger grid (a slab of a decomposed domain; else 0); the corner positions are computed at the larger
+ * grid's row indices so that they round as in the undecomposed model. RPL_ERR_STATE without
+ * SpatialAveraging. */
+int rpl_smooth_rows_async(rpl_handle* h, double dt, int64_t row0, int64_t nrows, int64_t y_offset);
 int rpl_sync(rpl_handle* h);
 /* Use the caller's CUDA stream (a cudaStream_t on the handle's device) instead of the handle's own. */
 int rpl_set_stream(rpl_handle* h, void* stream);

@@ -93,6 +93,7 @@ def lib():
         L.ora_pm_cells.argtypes = [_i64, _i64, _i64, _i64, _dp, _i64, _dp, _dp, _d, _dp, _dp, _dp, _d, _i32,
                                    _dp, _dp]
         L.ora_spatial_averaging.argtypes = [ctypes.POINTER(OraModel), _dp, _d]
+        L.ora_spatial_averaging_at.argtypes = [ctypes.POINTER(OraModel), _dp, _d, ctypes.c_int64]
         L.ora_num_threads.restype = ctypes.c_int
         L.ora_set_num_threads.argtypes = [ctypes.c_int]
         _lib = L
@@ -391,10 +392,12 @@ class Oracle:
         lib().ora_rk3_step(ctypes.byref(self.m), p(N), float(dt), int(nsteps), p(tt))
         return N, float(tt[0])
 
-    def spatial_averaging(self, N, dt):
-        """SpatialAveraging applied once (propagation_smoothing.jl:60-199)."""
+    def spatial_averaging(self, N, dt, y_offset=0):
+        """SpatialAveraging applied once (propagation_smoothing.jl:60-199); y_offset: the model's rows are
+        rows y_offset + 1 .. y_offset + Ny of a larger grid (a decomposition slab), whose row indices
+        the corner positions are computed at."""
         N = xfast(N).copy(order="F")
-        lib().ora_spatial_averaging(ctypes.byref(self.m), p(N), float(dt))
+        lib().ora_spatial_averaging_at(ctypes.byref(self.m), p(N), float(dt), int(y_offset))
         return N
 
     def stress_factor(self, N, t=0.0):

@@ -843,7 +843,12 @@ void ora_tendency(const ora_model* M, const double* N, double t, int32_t with_so
  * :163-199 (apply). Index arithmetic is 1-based like the reference so the bilinear weights round the
  * same way; a corner that one periodic wrap does not bring into range is clamped (the reference would
  * read its halo there; with a CFL-limited dt the corners stay within one cell). */
-void ora_spatial_averaging(const ora_model* M, double* N, double dt) {
+void ora_spatial_averaging(const ora_model* M, double* N, double dt) { ora_spatial_averaging_at(M, N, dt, 0); }
+
+/* The same with the model's rows at rows y_offset + 1 .. y_offset + Ny of a larger grid (a slab of a
+ * y-decomposed domain): corner positions and bilinear weights are computed at the larger grid's row
+ * indices, so they round as in the undecomposed run. */
+void ora_spatial_averaging_at(const ora_model* M, double* N, double dt, int64_t y_offset) {
     const int64_t Nx = M->Nx, Ny = M->Ny, Nk = M->Nk, Np = M->Np, P = Nx * Ny;
     const double g = 9.81;
     std::vector<double> cg(Nk), dcg(Nk), cs(Np), sn(Np);
@@ -878,10 +883,10 @@ void ora_spatial_averaging(const ora_model* M, double* N, double dt) {
                     for (int s1 = -1; s1 <= 1; s1 += 2)
                         for (int s2 = -1; s2 <= 1; s2 += 2) {
                             const double di = s1 * Ls_x + s2 * Ln_x, dj = s1 * Ls_y + s2 * Ln_y;
-                            const double ir = (double)i + di, jr = (double)j + dj;
+                            const double ir = (double)i + di, jr = (double)(j + y_offset) + dj;
                             const double fi = std::floor(ir), fj = std::floor(jr);
-                            const int64_t i0 = (int64_t)fi, j0 = (int64_t)fj;
-                            const double wi = ir - (double)i0, wj = jr - (double)j0;
+                            const int64_t i0 = (int64_t)fi, j0 = (int64_t)fj - y_offset;
+                            const double wi = ir - (double)i0, wj = jr - fj;
                             const int64_t i0c = wrap(i0, Nx, M->periodic_x), i1c = wrap(i0 + 1, Nx, M->periodic_x);
                             const int64_t j0c = wrap(j0, Ny, M->periodic_y), j1c = wrap(j0 + 1, Ny, M->periodic_y);
                             const double f00 = plane[(i0c - 1) + Nx * (j0c - 1)], f10 = plane[(i1c - 1) + Nx * (j0c - 1)];

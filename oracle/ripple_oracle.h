@@ -166,6 +166,8 @@ void ora_stress_factor(const ora_model* M, const double* N, double t, double* fa
 void ora_rk3_step(const ora_model* M, double* N, double dt, int64_t nsteps, double* t);
 /* SpatialAveraging applied once to N (x fastest) with the step's dt (propagation_smoothing.jl:60-199). */
 void ora_spatial_averaging(const ora_model* M, double* N, double dt);
+/* SpatialAveraging of a slab whose rows sit at rows y_offset + 1 .. y_offset + Ny of a larger grid. */
+void ora_spatial_averaging_at(const ora_model* M, double* N, double dt, int64_t y_offset);
 
 /* ---- diagnostics (src/Diagnostics) ---- */
 void ora_diagnostics(const ora_model* M, const double* N,

@@ -143,7 +143,8 @@ int check_error_word(Handle* h) {
 // One RK3 stage over rows [j_lo, j_hi): the stage's preparation kernels (wind, stress cap or learned
 // rows, pseudomomentum refresh, SourceTermSet rates; all column-local) when `prepare`, the stage kernel,
 // and when `finish` what completes the stage (after stage 3: SpatialAveraging and the clock).
-int launch_stage_rows(Handle* h, double dt, int stage, int64_t j_lo, int64_t j_hi, bool prepare, bool finish) {
+int launch_stage_rows(Handle* h, double dt, int stage, int64_t j_lo, int64_t j_hi, bool prepare, bool finish,
+                      bool defer_smooth = false) {
     cudaStream_t s = h->stream;
     const bool sources = h->has_sources && (h->src.wind_kind != RPL_WIND_NONE);
     const void* Nin = stage == 1 ? h->N : (stage == 2 ? h->A : h->B);
@@ -165,7 +166,8 @@ int launch_stage_rows(Handle* h, double dt, int stage, int64_t j_lo, int64_t j_h
         RPL_CUDA(rpl::launch_stage(*h, p, Nin, h->N, Nout, s));
     }
     if (finish && stage == 3) {
-        if (h->smooth) RPL_CUDA(rpl::launch_smooth(*h, h->A, h->N, dt, s));  // time_step.jl:168
+        if (h->smooth && !defer_smooth)
+            RPL_CUDA(rpl::launch_smooth(*h, h->A, h->N, dt, 0, h->desc.Ny, 0, s));  // time_step.jl:168
         h->time += dt;
         h->iteration += 1;
     }
@@ -822,9 +824,22 @@ int rpl_stage_rows_async(rpl_handle* hh, double dt, int32_t stage, int64_t row0,
     if ((st = check_step_args(h, dt))) return st;
     if (stage < 1 || stage > 3) return fail(RPL_ERR_ARGUMENT, "stage must be 1, 2 or 3");
     if (row0 < 0 || nrows < 0 || row0 + nrows > h->desc.Ny) return fail(RPL_ERR_ARGUMENT, "rows out of range");
-    if (flags & ~(RPL_STAGE_PREPARE | RPL_STAGE_FINISH)) return fail(RPL_ERR_ARGUMENT, "unknown stage flags");
+    if (flags & ~(RPL_STAGE_PREPARE | RPL_STAGE_FINISH | RPL_STAGE_DEFER_SMOOTH))
+        return fail(RPL_ERR_ARGUMENT, "unknown stage flags");
     return launch_stage_rows(h, dt, stage, row0, row0 + nrows, (flags & RPL_STAGE_PREPARE) != 0,
-                             (flags & RPL_STAGE_FINISH) != 0);
+                             (flags & RPL_STAGE_FINISH) != 0, (flags & RPL_STAGE_DEFER_SMOOTH) != 0);
+}
+
+int rpl_smooth_rows_async(rpl_handle* hh, double dt, int64_t row0, int64_t nrows, int64_t y_offset) {
+    int st = check_handle(hh);
+    if (st) return st;
+    Handle* h = reinterpret_cast<Handle*>(hh);
+    if ((st = check_step_args(h, dt))) return st;
+    if (!h->smooth) return fail(RPL_ERR_STATE, "the model has no SpatialAveraging");
+    if (row0 < 0 || nrows < 0 || row0 + nrows > h->desc.Ny) return fail(RPL_ERR_ARGUMENT, "rows out of range");
+    if (nrows == 0) return RPL_OK;
+    RPL_CUDA(rpl::launch_smooth(*h, h->A, h->N, dt, row0, row0 + nrows, y_offset, h->stream));
+    return RPL_OK;
 }
 
 int rpl_sync(rpl_handle* hh) {

@@ -227,7 +227,10 @@ void free_currents(Handle* h);
 // Waits for and releases the snapshot stream, events and staging buffer (rpl_output.cu).
 void free_output(Handle* h);
 // SpatialAveraging of the state Nin into Nout with the step's dt; release of its tables (rpl_smooth.cu).
-cudaError_t launch_smooth(Handle& h, const void* Nin, void* Nout, double dt, cudaStream_t s);
+// SpatialAveraging Nin -> Nout for rows [j_lo, j_hi) (all: 0, Ny); y_offset: the rows' offset in a larger
+// grid (a decomposition slab), at whose row indices the corner weights are computed (else 0).
+cudaError_t launch_smooth(Handle& h, const void* Nin, void* Nout, double dt, int64_t j_lo, int64_t j_hi,
+                          int64_t y_offset, cudaStream_t s);
 void free_smooth(Handle* h);
 
 // SourceTermSet rates of the action Nin into d_lin_rates; release of their buffers (rpl_terms.cu).

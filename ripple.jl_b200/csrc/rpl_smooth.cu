@@ -100,9 +100,10 @@ template <typename T>
 __global__ void __launch_bounds__(32 * ROWS)
 smooth_kernel(const T* __restrict__ Nin, T* __restrict__ Nout, int Nx, int Ny, int Nk, int Np,
               const T* __restrict__ W, const int* __restrict__ flag, const double* __restrict__ tab, double dphi,
-              double as, double an, double dt, double dx_inv, double dy_inv, int periodic_x, int periodic_y) {
-    const int j = blockIdx.y * ROWS + threadIdx.y + 1;  // 1-based like the reference
-    if (j > Ny) return;
+              double as, double an, double dt, double dx_inv, double dy_inv, int periodic_x, int periodic_y,
+              int j_lo, int j_hi, int y_offset) {
+    const int j = j_lo + blockIdx.y * ROWS + threadIdx.y + 1;  // 1-based like the reference, rows [j_lo, j_hi)
+    if (j > j_hi) return;
     const int n = blockIdx.z;
     const int i_first = blockIdx.x * STRIP + 1, i_last = min(i_first + STRIP - 1, Nx);
     const int64_t P = (int64_t)Nx * Ny;
@@ -117,9 +118,11 @@ smooth_kernel(const T* __restrict__ Nin, T* __restrict__ Nout, int Nx, int Ny, i
                 T acc = T(0);
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
-                    const double ir = (double)i + k.di[q], jr = (double)j + k.dj[q];
+                    // rows at their index in the larger grid of a decomposition slab (y_offset), so the
+                    // weights round as in the undecomposed model
+                    const double ir = (double)i + k.di[q], jr = (double)(j + y_offset) + k.dj[q];
                     const double fi = floor(ir), fj = floor(jr);
-                    const int i0 = (int)fi, j0 = (int)fj;
+                    const int i0 = (int)fi, j0 = (int)fj - y_offset;
                     const T wi = (T)(ir - fi), wj = (T)(jr - fj);
                     const int i0c = gse_index(i0, Nx, periodic_x), i1c = gse_index(i0 + 1, Nx, periodic_x);
                     const int j0c = gse_index(j0, Ny, periodic_y), j1c = gse_index(j0 + 1, Ny, periodic_y);
@@ -187,7 +190,8 @@ std::vector<double> smooth_tables(const Handle& h) {
 }
 
 template <typename T>
-cudaError_t launch_smooth_t(Handle& h, const void* Nin, void* Nout, double dt, cudaStream_t s) {
+cudaError_t launch_smooth_t(Handle& h, const void* Nin, void* Nout, double dt, int64_t j_lo, int64_t j_hi,
+                            int64_t y_offset, cudaStream_t s) {
     const rpl_desc& d = h.desc;
     const int Nk = (int)d.Nk, Np = (int)d.Np;
     const double* tab = (const double*)h.d_smooth;
@@ -201,18 +205,20 @@ cudaError_t launch_smooth_t(Handle& h, const void* Nin, void* Nout, double dt, c
         if (e != cudaSuccess) return e;
         h.smooth_dt = dt;
     }
-    const dim3 grid((unsigned)((d.Nx + STRIP - 1) / STRIP), (unsigned)((d.Ny + ROWS - 1) / ROWS), (unsigned)Np);
+    const dim3 grid((unsigned)((d.Nx + STRIP - 1) / STRIP), (unsigned)((j_hi - j_lo + ROWS - 1) / ROWS), (unsigned)Np);
     smooth_kernel<T><<<grid, dim3(32, ROWS), 0, s>>>((const T*)Nin, (T*)Nout, (int)d.Nx, (int)d.Ny, Nk, Np, W, flag,
                                                      tab, dphi, h.smooth_as, h.smooth_an, dt, 1.0 / d.dx,
-                                                     1.0 / d.dy, d.periodic_x, d.periodic_y);
+                                                     1.0 / d.dy, d.periodic_x, d.periodic_y, (int)j_lo, (int)j_hi,
+                                                     (int)y_offset);
     return cudaGetLastError();
 }
 
 }  // namespace
 
-cudaError_t launch_smooth(Handle& h, const void* Nin, void* Nout, double dt, cudaStream_t s) {
-    if (h.precision == RPL_FP64) return launch_smooth_t<double>(h, Nin, Nout, dt, s);
-    return launch_smooth_t<float>(h, Nin, Nout, dt, s);
+cudaError_t launch_smooth(Handle& h, const void* Nin, void* Nout, double dt, int64_t j_lo, int64_t j_hi,
+                          int64_t y_offset, cudaStream_t s) {
+    if (h.precision == RPL_FP64) return launch_smooth_t<double>(h, Nin, Nout, dt, j_lo, j_hi, y_offset, s);
+    return launch_smooth_t<float>(h, Nin, Nout, dt, j_lo, j_hi, y_offset, s);
 }
 
 void free_smooth(Handle* h) {

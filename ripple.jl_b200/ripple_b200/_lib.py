@@ -18,7 +18,7 @@ RPL_OK, RPL_ERR_ARGUMENT, RPL_ERR_DT, RPL_ERR_NONFINITE, RPL_ERR_CUDA, RPL_ERR_O
 RPL_FP64, RPL_FP32 = 0, 1
 RPL_F64, RPL_F32 = 0, 1
 RPL_LAYOUT_XFAST = 0
-RPL_STAGE_PREPARE, RPL_STAGE_FINISH = 1, 2
+RPL_STAGE_PREPARE, RPL_STAGE_FINISH, RPL_STAGE_DEFER_SMOOTH = 1, 2, 4
 RPL_TRANSPORT_NONE, RPL_TRANSPORT_REFRACTION, RPL_TRANSPORT_INTRINSIC = 0, 1, 2
 RPL_DEPTH_INFINITE, RPL_DEPTH_CONSTANT, RPL_DEPTH_FIELD = 0, 1, 2
 RPL_WIND_NONE, RPL_WIND_UNIFORM, RPL_WIND_HOLLAND, RPL_WIND_FIELD = 0, 1, 2, 3
@@ -96,6 +96,7 @@ _SIGNATURES = {
     "rpl_rows_get_on": (ctypes.c_int, [ctypes.c_void_p, _i32, _i64, _i64, ctypes.c_void_p, ctypes.c_void_p]),
     "rpl_rows_set_on": (ctypes.c_int, [ctypes.c_void_p, _i32, _i64, _i64, ctypes.c_void_p, ctypes.c_void_p]),
     "rpl_stage_rows_async": (ctypes.c_int, [ctypes.c_void_p, _d, _i32, _i64, _i64, _i32]),
+    "rpl_smooth_rows_async": (ctypes.c_int, [ctypes.c_void_p, _d, _i64, _i64, _i64]),
     "rpl_set_propagation_smoothing": (ctypes.c_int, [ctypes.c_void_p, _i32, _d, _d]),
     "rpl_diagnostics_device": (ctypes.c_int, [ctypes.c_void_p] + [ctypes.c_void_p] * 5),
     "rpl_snapshot_async": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, _i32]),

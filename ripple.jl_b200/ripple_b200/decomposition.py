@@ -13,8 +13,11 @@ nodes and spacings are the parent grid's own values, and the arithmetic per cell
 The exchange per stage: rows are copied out of the stage's input buffer into packed device buffers
 (rpl_rows_get), sent upward then downward with torch.distributed point-to-point operations (NCCL between
 GPUs; gloo between CPU processes in the tests), and copied into the halo rows (rpl_rows_set).
-Pseudomomentum coupling and SpatialAveraging are not decomposed (the averaging would need a halo
-exchange between stage 3 and the averaging).
+SpatialAveraging (propagation_smoothing.jl:60-199) averages each bin's field over the corners of a
+rectangle around every cell, after stage 3: stage 3 finishes without it (RPL_STAGE_DEFER_SMOOTH, its
+result stays in buffer A), A's halo rows are exchanged, and the owned rows are averaged
+(rpl_smooth_rows_async). The corners must stay within the 3 halo rows in y (smoothing_reach_rows < 3
+for the step's dt), which holds well inside the CFL limit. Pseudomomentum coupling is not decomposed.
 
 Overlap (rk3_steps_overlapped): an owned row r reads rows r-3 .. r+3, so the owned rows at least 3
 rows from either slab edge (local rows [6, ny)) read no halo row. Each stage first launches those
@@ -99,8 +102,6 @@ def local_workload(w, slab):
     g = w.grid
     if g.topology[1] != "Periodic":
         raise ArgumentError("the y-slab decomposition needs a periodic y axis")
-    if w.propagation_smoothing is not None:
-        raise ArgumentError("SpatialAveraging is not decomposed")
     if w.velocities is not None and not isinstance(w.velocities, dict):
         raise ArgumentError("only prescribed currents are decomposed")
     rows = slab.global_rows()
@@ -131,7 +132,37 @@ def local_workload(w, slab):
         sources = SourceTermSet(*local)
     return Workload(f"{w.name}[rows {slab.start}:{slab.stop}]", grid, w.spectral_grid, depth, N0, w.dt, w.nsteps,
                     velocities=vel, sources=sources, horizontal_advection=w.horizontal_advection,
-                    notes=dict(w.notes, slab=(slab.start, slab.stop)))
+                    notes=dict(w.notes, slab=(slab.start, slab.stop)),
+                    propagation_smoothing=w.propagation_smoothing)
+
+
+def smoothing_reach_rows(spectral_grid, smoothing, dt, dy):
+    """Largest |y offset| in rows of a SpatialAveraging corner for step dt (propagation_smoothing.jl:72-86,
+    117-158): |L_s sin(phi)| + |L_n cos(phi)| over dy, L_s = alpha_s |dc_g| dt, L_n = alpha_n c_g dphi dt,
+    with the deep-water c_g = sqrt(9.81 / kappa) / 2 and dc_g half its difference to the neighbouring rings."""
+    kappa = np.asarray(spectral_grid.κ, dtype=np.float64)
+    phi = np.asarray(spectral_grid.φ, dtype=np.float64)
+    pf = np.asarray(spectral_grid.φ_faces, dtype=np.float64)
+    cg = 0.5 * np.sqrt(9.81 / kappa)
+    lo = np.concatenate([cg[:1], cg[:-1]])
+    hi = np.concatenate([cg[1:], cg[-1:]])
+    dcg = np.abs(lo - hi) / 2.0
+    Ls = smoothing.αs * dcg * dt
+    Ln = smoothing.αn * cg * (pf[1] - pf[0]) * dt
+    reach = np.abs(Ls[:, None] * np.sin(phi)[None, :]) + np.abs(Ln[:, None] * np.cos(phi)[None, :])
+    return float(np.max(reach)) / float(dy)
+
+
+def check_smoothing_reach(w, dt, halo=HALO):
+    """ArgumentError when the averaging's corners would read beyond the halo rows for step dt."""
+    if w.propagation_smoothing is None:
+        return
+    yf = w.grid.yfaces()
+    dy = (yf[-1] - yf[0]) / w.grid.Ny
+    r = smoothing_reach_rows(w.spectral_grid, w.propagation_smoothing, dt, dy)
+    if not r < halo:
+        raise ArgumentError(f"SpatialAveraging corners reach {r:.3g} rows at dt = {dt}, beyond the {halo} halo rows "
+                            "of the y-slab decomposition")
 
 
 def interior_rows(slab):
@@ -178,12 +209,20 @@ class LibBackend:
         else:
             check(self.lib.rpl_rows_set(self.h, which, first, count, ptr))
 
-    def stage(self, dt, s):
-        check(self.lib.rpl_stage_async(self.h, float(dt), int(s)))
+    def stage(self, dt, s, defer_smooth=False):
+        if defer_smooth:
+            flags = _lib.RPL_STAGE_PREPARE | _lib.RPL_STAGE_FINISH | _lib.RPL_STAGE_DEFER_SMOOTH
+            check(self.lib.rpl_stage_rows_async(self.h, float(dt), int(s), 0, int(self.model.grid.Ny), flags))
+        else:
+            check(self.lib.rpl_stage_async(self.h, float(dt), int(s)))
 
-    def stage_rows(self, dt, s, first, count, prepare, finish):
-        flags = (_lib.RPL_STAGE_PREPARE if prepare else 0) | (_lib.RPL_STAGE_FINISH if finish else 0)
+    def stage_rows(self, dt, s, first, count, prepare, finish, defer_smooth=False):
+        flags = ((_lib.RPL_STAGE_PREPARE if prepare else 0) | (_lib.RPL_STAGE_FINISH if finish else 0) |
+                 (_lib.RPL_STAGE_DEFER_SMOOTH if defer_smooth else 0))
         check(self.lib.rpl_stage_rows_async(self.h, float(dt), int(s), int(first), int(count), flags))
+
+    def smooth_rows(self, dt, first, count, y_offset=0):
+        check(self.lib.rpl_smooth_rows_async(self.h, float(dt), int(first), int(count), int(y_offset)))
 
     def mark_input(self):
         """The stage's input is final on the compute stream (before the interior launch)."""
@@ -250,11 +289,24 @@ def exchange_local(backends, slabs, which, bufs):
         b.rows_set(which, *s.halo_high(), q["recv_high"])
 
 
-def rk3_steps_overlapped(backends, slabs, exchange, dt, nsteps, before_step=None):
+def _smooth(backends, slabs, exchange, dt):
+    """SpatialAveraging of a decomposed step: stage 3's result (buffer A) gets its halo rows from the
+    neighbours, then every slab averages its owned rows into N."""
+    for b in backends:
+        b.mark_input()
+        b.begin_exchange()
+    exchange(1)
+    for b, sl in zip(backends, slabs):
+        b.end_exchange()
+        b.smooth_rows(dt, sl.halo, sl.ny, sl.start - sl.halo)
+
+
+def rk3_steps_overlapped(backends, slabs, exchange, dt, nsteps, before_step=None, smooth=False):
     """nsteps decomposed SSP-RK3 steps with the exchange beside the interior rows: per stage every slab
     launches its interior rows (with the stage's preparation kernels), the halos of the stage's input
     are exchanged (exchange(which), between the backends' begin_exchange and end_exchange), then every
-    slab launches its two boundary row ranges (the last one finishes the stage)."""
+    slab launches its two boundary row ranges (the last one finishes the stage). smooth: the models have
+    SpatialAveraging, applied after stage 3 (see _smooth)."""
     for _ in range(nsteps):
         if before_step is not None:
             before_step()
@@ -270,21 +322,26 @@ def rk3_steps_overlapped(backends, slabs, exchange, dt, nsteps, before_step=None
                 b.end_exchange()
                 (l0, l1), (h0, h1) = boundary_rows(sl)
                 b.stage_rows(dt, s, l0, l1 - l0, False, False)
-                b.stage_rows(dt, s, h0, h1 - h0, False, True)
+                b.stage_rows(dt, s, h0, h1 - h0, False, True, defer_smooth=smooth and s == 3)
+        if smooth:
+            _smooth(backends, slabs, exchange, dt)
     for b in backends:
         b.sync()
 
 
-def rk3_steps(backends, exchange, dt, nsteps, before_step=None):
+def rk3_steps(backends, exchange, dt, nsteps, before_step=None, slabs=None):
     """nsteps decomposed SSP-RK3 steps: before stage s the halo rows of its input buffer (N, A, B) are
-    exchanged, then every slab runs the stage."""
+    exchanged, then every slab runs the stage. slabs (given for models with SpatialAveraging): the
+    averaging after stage 3 (see _smooth)."""
     for _ in range(nsteps):
         if before_step is not None:
             before_step()
         for s, which in ((1, 0), (2, 1), (3, 2)):
             exchange(which)
             for b in backends:
-                b.stage(dt, s)
+                b.stage(dt, s, defer_smooth=slabs is not None and s == 3)
+        if slabs is not None:
+            _smooth(backends, slabs, exchange, dt)
     for b in backends:
         b.sync()
 
@@ -317,16 +374,18 @@ class DecomposedModel:
         m = self.model
         check(m._lib.rpl_set_clock(m.handle, m.clock.time, m.clock.iteration))
         before = m._push_field_wind if m._field_wind is not None else None
+        check_smoothing_reach(self.local, dt)
+        smooth = self.local.propagation_smoothing is not None
         with torch.cuda.stream(self.stream):
             if self.overlap:
                 rk3_steps_overlapped([self.backend], [self.slab],
                                      lambda which: exchange_dist(self.backend, self.slab, which, self.bufs,
                                                                  self.group, self.xstream),
-                                     dt, nsteps, before_step=before)
+                                     dt, nsteps, before_step=before, smooth=smooth)
             else:
                 rk3_steps([self.backend],
                           lambda which: exchange_dist(self.backend, self.slab, which, self.bufs, self.group),
-                          dt, nsteps, before_step=before)
+                          dt, nsteps, before_step=before, slabs=[self.slab] if smooth else None)
         m.clock.last_Δt = dt
         return self
 

@@ -28,6 +28,7 @@ class OracleBackend:
     def __init__(self, oracle_mod, w):
         import torch  # noqa: F401
         self.o = oracle_mod.Oracle(w)
+        self.smooth = w.propagation_smoothing is not None   # stage 3 into A, then the averaging A -> N
         self.N = np.asfortranarray(np.array(w.N0, dtype=np.float64))
         self.A = np.zeros_like(self.N, order="F")
         self.B = np.zeros_like(self.N, order="F")
@@ -45,18 +46,11 @@ class OracleBackend:
         Nx, _, Nk, Np = self.N.shape
         self._arr(which)[:, first:first + count] = buf.numpy().reshape(Np, count, Nx, Nk).transpose(2, 1, 3, 0)
 
-    def stage(self, dt, s):
-        if s == 1:
-            self.A[...] = relu(self.N + dt * self.o.tendency(self.N, self.t))
-        elif s == 2:
-            st = relu(self.A + dt * self.o.tendency(self.A, self.t))
-            self.B[...] = relu(0.75 * self.N + 0.25 * st)
-        else:
-            st = relu(self.B + dt * self.o.tendency(self.B, self.t))
-            self.N[...] = relu((1.0 / 3.0) * self.N + (2.0 / 3.0) * st)
-            self.t += dt
+    def stage(self, dt, s, defer_smooth=False):
+        Ny = self.N.shape[1]
+        self.stage_rows(dt, s, 0, Ny, True, True, defer_smooth)
 
-    def stage_rows(self, dt, s, first, count, prepare, finish):
+    def stage_rows(self, dt, s, first, count, prepare, finish, defer_smooth=False):
         """The stage for rows [first, first + count) only, from the buffers as they are now (halo rows
         included, refreshed or not), like rpl_stage_rows_async."""
         if count > 0:
@@ -68,9 +62,17 @@ class OracleBackend:
                 self.B[:, r] = relu(0.75 * self.N + 0.25 * st)[:, r]
             else:
                 st = relu(self.B + dt * self.o.tendency(self.B, self.t))
-                self.N[:, r] = relu((1.0 / 3.0) * self.N + (2.0 / 3.0) * st)[:, r]
+                out = self.A if self.smooth else self.N
+                out[:, r] = relu((1.0 / 3.0) * self.N + (2.0 / 3.0) * st)[:, r]
         if finish and s == 3:
+            if self.smooth and not defer_smooth:
+                self.smooth_rows(dt, 0, self.N.shape[1])
             self.t += dt
+
+    def smooth_rows(self, dt, first, count, y_offset=0):
+        """SpatialAveraging A -> N for rows [first, first + count), like rpl_smooth_rows_async."""
+        r = slice(first, first + count)
+        self.N[:, r] = self.o.spatial_averaging(self.A, dt, y_offset)[:, r]
 
     def mark_input(self):
         pass
@@ -87,9 +89,17 @@ class OracleBackend:
 
 def cases():
     from test_source_terms import random_terms_workload
+    smoothed = workloads.seamount_eddies(N=24, Nz=8, Nk=8, Np=12, nsteps=3)
+    smoothed.propagation_smoothing = rp.SpatialAveraging(αs=0.5, αn=0.5)
     return [workloads.seamount_eddies(N=24, Nz=8, Nk=8, Np=12, nsteps=3),   # currents, depth field
             workloads.hurricane_swell(N=24, Nk=8, Np=12, nsteps=3),          # sources, moving storm
-            random_terms_workload(N=12, Nk=8, Np=12)]                        # SourceTermSet, a rate field
+            random_terms_workload(N=12, Nk=8, Np=12),                        # SourceTermSet, a rate field
+            smoothed]                                                        # SpatialAveraging after every step
+
+
+def smoothing_slabs(w, slabs):
+    """The slabs argument of rk3_steps for models with SpatialAveraging, else None."""
+    return slabs if w.propagation_smoothing is not None else None
 
 
 def _buffers(slab, w):
@@ -124,10 +134,6 @@ def test_local_grid_keeps_the_parent_geometry():
 
 def test_local_workload_rejects_what_is_not_decomposed():
     s = dc.Slab(24, 2, 0)
-    w = cases()[0]
-    w.propagation_smoothing = rp.SpatialAveraging()
-    with pytest.raises(rp.ArgumentError):
-        dc.local_workload(w, s)                       # the averaging needs an exchange after stage 3
     w = workloads.self_coupled_swell(N=24, Nk=8, Np=12)
     with pytest.raises(rp.ArgumentError):
         dc.local_workload(w, s)                       # pseudomomentum coupling
@@ -139,20 +145,33 @@ def test_local_workload_rejects_what_is_not_decomposed():
         dc.local_workload(w, s)                       # a bounded y axis
 
 
-@pytest.mark.parametrize("case", [0, 1])
+def test_smoothing_reach_limits_the_step():
+    """The averaging's corners must stay within the 3 halo rows: at the workload's dt they reach a small
+    fraction of a row; a dt that takes them 3 rows or further is refused."""
+    w = cases()[3]
+    dy = (w.grid.yfaces()[-1] - w.grid.yfaces()[0]) / w.grid.Ny
+    r = dc.smoothing_reach_rows(w.spectral_grid, w.propagation_smoothing, w.dt, dy)
+    assert 0 < r < 1
+    dc.check_smoothing_reach(w, w.dt)
+    with pytest.raises(rp.ArgumentError):
+        dc.check_smoothing_reach(w, w.dt * 3.01 / r)
+
+
+@pytest.mark.parametrize("case", [0, 1, 3])
 @pytest.mark.parametrize("world", [2, 3])
 def test_oracle_slabs_in_one_process_equal_the_global_run(oracle_mod, case, world):
     w = cases()[case]
     slabs = [dc.Slab(w.grid.Ny, world, r) for r in range(world)]
     backs = [OracleBackend(oracle_mod, dc.local_workload(w, s)) for s in slabs]
     bufs = [_buffers(s, w) for s in slabs]
-    dc.rk3_steps(backs, lambda which: dc.exchange_local(backs, slabs, which, bufs), w.dt, 3)
+    dc.rk3_steps(backs, lambda which: dc.exchange_local(backs, slabs, which, bufs), w.dt, 3,
+                 slabs=smoothing_slabs(w, slabs))
     got = np.concatenate([b.N[:, s.owned()] for b, s in zip(backs, slabs)], axis=1)
     ref, _ = oracle_mod.Oracle(w).step(w.N0, w.dt, 3)
     assert np.array_equal(got, ref)
 
 
-@pytest.mark.parametrize("case", [0, 1, 2])
+@pytest.mark.parametrize("case", [0, 1, 2, 3])
 @pytest.mark.parametrize("world", [1, 2, 3])
 def test_oracle_overlapped_slabs_equal_the_global_run(oracle_mod, case, world):
     """Interior rows computed before the exchange (their halo rows still hold the previous stage's
@@ -165,7 +184,8 @@ def test_oracle_overlapped_slabs_equal_the_global_run(oracle_mod, case, world):
             arr[:, :3] = -7.0
             arr[:, -3:] = -7.0
     bufs = [_buffers(s, w) for s in slabs]
-    dc.rk3_steps_overlapped(backs, slabs, lambda which: dc.exchange_local(backs, slabs, which, bufs), w.dt, 3)
+    dc.rk3_steps_overlapped(backs, slabs, lambda which: dc.exchange_local(backs, slabs, which, bufs), w.dt, 3,
+                            smooth=w.propagation_smoothing is not None)
     got = np.concatenate([b.N[:, s.owned()] for b, s in zip(backs, slabs)], axis=1)
     ref, _ = oracle_mod.Oracle(w).step(w.N0, w.dt, 3)
     assert np.array_equal(got, ref)
@@ -193,11 +213,13 @@ def _gloo_rank(rank, world, port, case, out, overlap=False):
         slab = dc.Slab(w.grid.Ny, world, rank)
         back = OracleBackend(oracle_mod, dc.local_workload(w, slab))
         bufs = _buffers(slab, w)
+        smooth = w.propagation_smoothing is not None
         if overlap:
             dc.rk3_steps_overlapped([back], [slab], lambda which: dc.exchange_dist(back, slab, which, bufs),
-                                    w.dt, 3)
+                                    w.dt, 3, smooth=smooth)
         else:
-            dc.rk3_steps([back], lambda which: dc.exchange_dist(back, slab, which, bufs), w.dt, 3)
+            dc.rk3_steps([back], lambda which: dc.exchange_dist(back, slab, which, bufs), w.dt, 3,
+                         slabs=[slab] if smooth else None)
         parts = [None] * world
         dist.all_gather_object(parts, (slab.start, back.N[:, slab.owned()]))
         if rank == 0:
@@ -213,7 +235,7 @@ def _free_port():
 
 
 @pytest.mark.parametrize("world,case,overlap", [(2, 0, False), (3, 0, False), (2, 1, False), (2, 0, True),
-                                                 (3, 1, True)])
+                                                 (3, 1, True), (2, 3, False), (3, 3, True)])
 def test_oracle_slabs_across_gloo_ranks_equal_the_global_run(oracle_mod, tmp_path, world, case, overlap):
     import torch.multiprocessing as mp
     out = str(tmp_path / "global.npy")
@@ -227,7 +249,7 @@ def test_oracle_slabs_across_gloo_ranks_equal_the_global_run(oracle_mod, tmp_pat
 # ---------------------------------------------------------------- CUDA path (GPU)
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", [0, 1])
+@pytest.mark.parametrize("case", [0, 1, 3])
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 @pytest.mark.parametrize("world", [2, 3])
 def test_library_slabs_on_one_gpu_equal_the_global_model(case, precision, world):
@@ -247,7 +269,8 @@ def test_library_slabs_on_one_gpu_equal_the_global_model(case, precision, world)
              for k in ("send_low", "send_high", "recv_low", "recv_high")} for _ in slabs]
 
     with torch.cuda.stream(st):
-        dc.rk3_steps(backs, lambda which: dc.exchange_local(backs, slabs, which, bufs), w.dt, 3)
+        dc.rk3_steps(backs, lambda which: dc.exchange_local(backs, slabs, which, bufs), w.dt, 3,
+                     slabs=smoothing_slabs(w, slabs))
     got = np.concatenate([m.action.interior()[:, s.owned()] for m, s in zip(models, slabs)], axis=1)
     g = w.model(precision)
     rp.time_step(g, w.dt, 3)
@@ -256,12 +279,14 @@ def test_library_slabs_on_one_gpu_equal_the_global_model(case, precision, world)
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("case", [0, 3])
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
-def test_library_overlapped_slabs_on_one_gpu_equal_the_global_model(precision):
+def test_library_overlapped_slabs_on_one_gpu_equal_the_global_model(case, precision):
     """Row-range stage launches (interior rows, then the two boundary ranges) on one compute stream, the
-    exchange copies on a second stream ordered by events, halo rows never recomputed."""
+    exchange copies on a second stream ordered by events, halo rows never recomputed; with
+    SpatialAveraging (case 3) the averaging after the exchange of stage 3's result."""
     import torch
-    w = cases()[0]
+    w = cases()[case]
     if precision == "fp32":
         w.N0 = w.N0.astype(np.float32, order="F")
     world = 2
@@ -281,7 +306,7 @@ def test_library_overlapped_slabs_on_one_gpu_equal_the_global_model(precision):
             dc.exchange_local(backs, slabs, which, bufs)
 
     with torch.cuda.stream(st):
-        dc.rk3_steps_overlapped(backs, slabs, exchange, w.dt, 3)
+        dc.rk3_steps_overlapped(backs, slabs, exchange, w.dt, 3, smooth=w.propagation_smoothing is not None)
     got = np.concatenate([m.action.interior()[:, s.owned()] for m, s in zip(models, slabs)], axis=1)
     g = w.model(precision)
     rp.time_step(g, w.dt, 3)
@@ -290,10 +315,11 @@ def test_library_overlapped_slabs_on_one_gpu_equal_the_global_model(precision):
 
 
 @pytest.mark.gpu
-def test_one_rank_decomposed_model_equals_the_global_model():
+@pytest.mark.parametrize("case", [1, 3])
+def test_one_rank_decomposed_model_equals_the_global_model(case):
     import datetime
     import torch.distributed as dist
-    w = cases()[1]
+    w = cases()[case]
     store = dist.TCPStore("127.0.0.1", _free_port(), 1, True)
     dist.init_process_group("gloo", store=store, rank=0, world_size=1, timeout=datetime.timedelta(seconds=60))
     try:
