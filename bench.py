@@ -98,8 +98,8 @@ WORKLOAD_NAMES = {"seamount": "seamount_eddies", "hurricane": "hurricane_swell",
                   "learned": "hurricane_swell (learned source)", "selfcoupled": "self_coupled_swell"}
 TRAFFIC_SUFFIX = {"seamount": "", "hurricane": "_hurricane", "selfcoupled": "_selfcoupled"}
 # the FP32 stage kernels each workload runs (refraction: two passes per stage; intrinsic: one fused kernel)
-STAGE_KERNELS = {"seamount": "xy_kernel+kp_kernel", "hurricane": "tile_kernel",
-                 "selfcoupled": "xy_kernel+kp_kernel"}
+STAGE_KERNELS = {"seamount": "xyw_kernel+kq_kernel", "hurricane": "tile_kernel",
+                 "selfcoupled": "xyw_kernel+kq_kernel"}
 DATA = {"seamount": "synthetic (seeded seamount depth, eddy currents, JONSWAP-like N0)",
         "hurricane": "synthetic (Holland hurricane on a linear track, uniform N0 = 1e-6)",
         "selfcoupled": "synthetic (Gaussian swell packet, 50 m depth, pseudomomentum self-coupling)"}
