@@ -262,7 +262,8 @@ int rpl_create(const rpl_desc* d, rpl_handle** out) {
     const int64_t c3 = d->Nx * d->Ny * d->Nk, P = d->Nx * d->Ny, nb = d->Nk * d->Np;
     int64_t need = 3 * units * (int64_t)elem + 16 * c3 * 8 + (d->depth_kind == RPL_DEPTH_FIELD ? (c3 + P) * 8 : 0) +
                    (4 * P + 2 * (d->Nx + d->Ny)) * 8 + 6 * P * 8 + 8 * nb * 8 +
-                   (d->precision == RPL_FP32 && d->transport == RPL_TRANSPORT_REFRACTION ? units * 4 + 3 * c3 * 4 : 0);
+                   (d->precision == RPL_FP32 && d->transport == RPL_TRANSPORT_REFRACTION ? units * 4 + 3 * c3 * 4 : 0) +
+                   (d->precision == RPL_FP32 && d->transport == RPL_TRANSPORT_INTRINSIC ? c3 * 4 : 0);
     if (d->memory_limit_bytes > 0 && need > d->memory_limit_bytes)
         return fail(RPL_ERR_OOM, "model needs " + std::to_string(need) + " device bytes, above the memory limit of " +
                                      std::to_string(d->memory_limit_bytes));
@@ -399,8 +400,11 @@ int rpl_create(const rpl_desc* d, rpl_handle** out) {
     TRY(dalloc(h, &h->d_bin32, 8 * d->Nk));
     if (d->transport == RPL_TRANSPORT_REFRACTION && rpl::tile32_supported(*h) && !h->force_column_kernel)
         TRY(dalloc(h, &h->d_sxy, units));  // the two-pass refraction stage of FP32 models
-    if (h->d_sxy && rpl::xyw_supported(*h) && !h->pass_a_tiles) {   // its y-walk pass A: FP32 velocity planes, upwind ratios
-        TRY(dalloc(h, &h->d_vel32, 3 * c3));
+    const bool intrinsic32 = d->transport == RPL_TRANSPORT_INTRINSIC && rpl::tile32_supported(*h) &&
+                             !h->force_column_kernel;
+    if ((h->d_sxy || intrinsic32) && rpl::xyw_supported(*h) && !h->pass_a_tiles) {
+        // the y-walk x/y kernels: FP32 velocity planes (intrinsic: c_g only) and upwind ratios
+        TRY(dalloc(h, &h->d_vel32, (h->d_sxy ? 3 : 1) * c3));
         h->vel_regions = rpl::xyw_regions(*h);
         TRY(dalloc(h, &h->d_rmax, 2 * h->vel_regions * d->Nk));
     }

@@ -276,6 +276,9 @@ int64_t xyw_regions(const Handle& h);             // regions of the upwind ratio
 // d_vel32).
 cudaError_t launch_vel32(const Handle& h, cudaStream_t s);
 cudaError_t launch_xyw(const TileArgs& a, cudaStream_t s);   // writes a.sxy for rows [j_lo, j_hi)
+// The whole stage of intrinsic transport (no currents) without sources (src 0) or with the SourceTermSet
+// rates (src 3, the tile body's SRC).
+cudaError_t launch_xyi(const TileArgs& a, int src, cudaStream_t s);
 
 // ---- FP32 tiled stage kernel (rpl_tile32.cu) ----
 bool tile32_supported(const Handle& h);

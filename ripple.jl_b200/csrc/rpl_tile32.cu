@@ -870,6 +870,8 @@ cudaError_t launch_L(const Handle& h, const StageParams& p, const TileArgs& a, c
         if (src == 2) return launch_variant<L, true, 2>(a, tiles, s);
         return src ? launch_variant<L, true, 1>(a, tiles, s) : launch_variant<L, true, 0>(a, tiles, s);
     }
+    // the y-walk form (rpl_xyw.cu, one reconstruction per face) without the bundle or learned sources
+    if (a.rmax && (src == 0 || src == 3)) return launch_xyi(a, src, s);
     if (src == 3) return launch_variant<L, false, 3>(a, tiles, s);
     if (src == 2) return launch_variant<L, false, 2>(a, tiles, s);
     return src ? launch_variant<L, false, 1>(a, tiles, s) : launch_variant<L, false, 0>(a, tiles, s);
@@ -929,9 +931,13 @@ TileArgs make_tile_args(const Handle& h, const StageParams& p, const void* Nin, 
     a.pass_b_quads = !h.pass_b_pairs;
     if (h.d_vel32) {
         const int64_t c3 = h.desc.Nx * h.desc.Ny * h.desc.Nk;
-        a.ux32 = h.d_vel32;
-        a.uy32 = h.d_vel32 + c3;
-        a.cgc32 = h.d_vel32 + 2 * c3;
+        if (h.desc.transport == RPL_TRANSPORT_REFRACTION) {
+            a.ux32 = h.d_vel32;
+            a.uy32 = h.d_vel32 + c3;
+            a.cgc32 = h.d_vel32 + 2 * c3;
+        } else {
+            a.cgc32 = h.d_vel32;   // intrinsic transport: the c_g plane only
+        }
         a.rmax = h.d_rmax;
     }
     return a;

@@ -309,6 +309,35 @@ def test_fp32_pass_b_forms_agree_bitwise(monkeypatch, shape, current, depth_fiel
     assert np.array_equal(out[""], out["pairs"])
 
 
+def intrinsic_workloads():
+    from test_source_terms import random_terms_workload
+    plain = workloads.seamount_eddies(N=40, Nz=8, Nk=16, Np=24, nsteps=3)
+    plain.velocities = None                           # intrinsic transport, c_g per cell (depth field)
+    return {"depth_field": plain,
+            "hurricane": workloads.hurricane_swell(N=48, Nk=32, Np=36, nsteps=3),     # bundle, stress cap
+            "hurricane_small_k": workloads.hurricane_swell(N=33, Nk=8, Np=12, nsteps=3),
+            "terms": random_terms_workload(N=37, Nk=16, Np=24)}                       # SourceTermSet rates
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["depth_field", "hurricane", "hurricane_small_k", "terms"])
+def test_fp32_intrinsic_forms_agree_bitwise(monkeypatch, name):
+    """The y-walk stage of intrinsic transport (one reconstruction per x and y face, the SourceTermSet rates
+    and the stage update in the same kernel) and the fused tile kernel (RPL_PASS_A=tiles) give the same
+    FP32 state bit for bit after three SSP-RK3 steps; the bundle sources (hurricane) take the tile kernel
+    in both."""
+    w = intrinsic_workloads()[name]
+    out = {}
+    for form in ("", "tiles"):
+        monkeypatch.setenv("RPL_PASS_A", form)
+        m = w.model("fp32")
+        rp.time_step(m, w.dt, 3)
+        out[form] = m.action.interior()
+        m.close()
+    assert np.all(np.isfinite(out[""])) and np.max(np.abs(out[""])) > 0
+    assert np.array_equal(out[""], out["tiles"])
+
+
 @pytest.mark.parametrize("column_kernel", ["0", "1"])
 def test_fp32_kernels_intrinsic_and_depth_field(oracle_mod, monkeypatch, column_kernel):
     monkeypatch.setenv("RPL_FORCE_COLUMN_KERNEL", column_kernel)
