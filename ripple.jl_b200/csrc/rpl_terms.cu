@@ -41,6 +41,20 @@ struct TermsArgs {
     const double* weights;  // (Nk, Np) spectral cell measures
 };
 
+// x^e for x >= 0: small integer powers by products (x^0 = 1, including 0^0 as the reference's ^;
+// x^1 = x exactly), others by pow. The wave-age input's default power is 1 (Sources.jl:77-84).
+__device__ __forceinline__ double pow_nonneg(double x, double e) {
+    if (e == 1.0) return x;
+    if (e == 0.0) return 1.0;
+    if (e == 2.0) return x * x;
+    if (e == 3.0) return x * x * x;
+    if (e == 4.0) {
+        const double x2 = x * x;
+        return x2 * x2;
+    }
+    return pow(x, e);
+}
+
 __device__ __forceinline__ double warp_sum(double v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
@@ -48,61 +62,64 @@ __device__ __forceinline__ double warp_sum(double v) {
 
 template <typename T>
 __global__ void __launch_bounds__(256) terms_kernel(const T* __restrict__ N, TermsArgs a, T* __restrict__ R) {
+    // each column's per-term values (x0, x1) for the bin pass, one slot per warp: no per-thread arrays
+    // indexed by the runtime term number (those would live in local memory)
+    __shared__ double2 cell[256 / 32][RPL_MAX_TERMS];
     const int64_t c = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     if (c >= a.P) return;  // uniform per warp
     const int64_t Nk = a.Nk, Np = a.Np, nb = Nk * Np;
-    // pass 1: per-column integrals
+    // pass 1: m0 = sum N w over the column
     double m0 = 0.0;
-    double sk[RPL_MAX_TERMS], ss[RPL_MAX_TERMS], sd[RPL_MAX_TERMS];
-    for (int t = 0; t < a.n; ++t) sk[t] = ss[t] = sd[t] = 0.0;
     for (int64_t n = 0; n < Np; ++n)
-        for (int64_t m = lane; m < Nk; m += 32) {
-            const double v = (double)N[(n * a.P + c) * Nk + m];
-            const int64_t b = m + Nk * n;
-            m0 += v * a.weights[b];
-            if (v > 0.0)
-                for (int t = 0; t < a.n; ++t)
-                    if (a.kind[t] == RPL_TERM_MEAN_SPECTRUM) {
-                        const double* tb = a.tabs + (int64_t)t * TABS * nb;
-                        sk[t] += v * tb[nb + b];
-                        ss[t] += v * tb[2 * nb + b];
-                        sd[t] += v * tb[3 * nb + b];
-                    }
-        }
+        for (int64_t m = lane; m < Nk; m += 32)
+            m0 += (double)N[(n * a.P + c) * Nk + m] * a.weights[m + Nk * n];
     m0 = warp_sum(m0);
-    // per-cell values of each term: (x0, x1)
-    double x0[RPL_MAX_TERMS], x1[RPL_MAX_TERMS];
+    // per-cell values of each term: (x0, x1); a mean-spectrum term sums its column integrals first
     for (int t = 0; t < a.n; ++t) {
         const double rate = a.rate_field[t] ? a.rate_field[t][c] : a.rate[t];
-        x0[t] = x1[t] = 0.0;
+        double x0 = 0.0, x1 = 0.0;
         switch (a.kind[t]) {
             case RPL_TERM_EXPONENTIAL_WIND:
-                x0[t] = rate;
+                x0 = rate;
                 break;
             case RPL_TERM_WAVE_AGE_WIND:
-                x0[t] = rate;
-                x1[t] = a.speed_field[t] ? a.speed_field[t][c] : a.speed[t];
+                x0 = rate;
+                x1 = a.speed_field[t] ? a.speed_field[t][c] : a.speed[t];
                 break;
             case RPL_TERM_WHITECAPPING: {
                 const double excess = fmax(m0 / a.p[t][0] - 1.0, 0.0);
-                x0[t] = rate * pow(excess, a.p[t][1]);
+                x0 = rate * pow(excess, a.p[t][1]);
                 break;
             }
             default: {  // mean spectrum: x0 = -C_ds (m0 kbar^2)^2 sigmabar, x1 = kbar (0: no dissipation)
-                const double num_k = warp_sum(sk[t]), num_s = warp_sum(ss[t]), den = warp_sum(sd[t]);
+                const double* tb = a.tabs + (int64_t)t * TABS * nb;
+                double sk = 0.0, ss = 0.0, sd = 0.0;
+                for (int64_t n = 0; n < Np; ++n)
+                    for (int64_t m = lane; m < Nk; m += 32) {
+                        const double v = (double)N[(n * a.P + c) * Nk + m];
+                        const int64_t b = m + Nk * n;
+                        if (v > 0.0) {
+                            sk += v * tb[nb + b];
+                            ss += v * tb[2 * nb + b];
+                            sd += v * tb[3 * nb + b];
+                        }
+                    }
+                const double num_k = warp_sum(sk), num_s = warp_sum(ss), den = warp_sum(sd);
                 const double q = a.p[t][3];
                 const double kbar = den > 0.0 ? pow(num_k / den, 1.0 / q) : 0.0;
                 const double sbar = den > 0.0 ? pow(num_s / den, 1.0 / q) : 0.0;
                 if (m0 > 0.0 && kbar > 0.0) {
                     const double alpha = m0 * kbar * kbar;
-                    x0[t] = -a.p[t][0] * alpha * alpha * sbar;
-                    x1[t] = kbar;
+                    x0 = -a.p[t][0] * alpha * alpha * sbar;
+                    x1 = kbar;
                 }
                 break;
             }
         }
+        if (lane == 0) cell[w][t] = make_double2(x0, x1);
     }
+    __syncwarp();
     // pass 2: the rate of every bin
     for (int64_t n = 0; n < Np; ++n)
         for (int64_t m = lane; m < Nk; m += 32) {
@@ -110,26 +127,27 @@ __global__ void __launch_bounds__(256) terms_kernel(const T* __restrict__ N, Ter
             double r = 0.0;
             for (int t = 0; t < a.n; ++t) {
                 const double* tb = a.tabs + (int64_t)t * TABS * nb;
+                const double2 x = cell[w][t];
                 switch (a.kind[t]) {
                     case RPL_TERM_EXPONENTIAL_WIND:
-                        r += x0[t] * tb[b];
+                        r += x.x * tb[b];
                         break;
                     case RPL_TERM_WAVE_AGE_WIND: {
                         const double al = tb[b];
                         if (al > 0.0) {
-                            const double excess = fmax(x1[t] * al * tb[nb + b] - a.p[t][0], 0.0);
-                            r += x0[t] * pow(excess, a.p[t][1]) * tb[2 * nb + b];
+                            const double excess = fmax(x.y * al * tb[nb + b] - a.p[t][0], 0.0);
+                            r += x.x * pow_nonneg(excess, a.p[t][1]) * tb[2 * nb + b];
                         }
                         break;
                     }
                     case RPL_TERM_WHITECAPPING:
-                        r -= x0[t] * tb[b];
+                        r -= x.x * tb[b];
                         break;
                     default: {
                         const double k = tb[b];
-                        if (x1[t] > 0.0 && k > 0.0) {
-                            const double ratio = k / x1[t];
-                            r -= x0[t] * (a.p[t][1] * ratio + a.p[t][2] * ratio * ratio);
+                        if (x.y > 0.0 && k > 0.0) {
+                            const double ratio = k / x.y;
+                            r -= x.x * (a.p[t][1] * ratio + a.p[t][2] * ratio * ratio);
                         }
                         break;
                     }
