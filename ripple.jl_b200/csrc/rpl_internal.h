@@ -195,6 +195,7 @@ struct Handle {
     rpl_source_term terms[RPL_MAX_TERMS] = {};  // field pointers refer to d_terms_fields
     void* d_lin_rates = nullptr;   // per cell-bin rate, state layout and type
     double* d_terms = nullptr;     // per term 3 bin tables (Nk*Np each) then the copied fields
+    double2* d_tcol = nullptr;     // per (i,j) column and term the stage's per-cell term values (x0, x1)
     int64_t terms_bytes = 0;
     // diagnostics scratch
     double* d_diag = nullptr;      // 5 (Nx,Ny) fields + block partials

@@ -4,7 +4,9 @@
 // Before every stage (and for rpl_tendency) terms_kernel turns the stage's action into one rate per
 // cell-bin, R(i,j,m,n) = sum over terms of +rate (wind input, split_growth_rate) or -rate (dissipation,
 // split_damping_rate) (src/Sources/Sources.jl:430-434,443-449), written in the state's layout and type;
-// the stage kernels then add R * N to the tendency. One warp per (i,j) column, lanes over kappa bins:
+// the stage kernels then add R * N to the tendency. With up to 4 terms, terms_cols_kernel and
+// terms_bins_kernel (below) split the work by column and by bin; otherwise terms_kernel does both passes
+// in one warp per (i,j) column, lanes over kappa bins:
 //   pass 1 sums the column's integrals in FP64: m0 = sum N w over every bin (local_zeroth_moment,
 //     Sources.jl:1471-1480) and, per MeanSpectrumWhitecapping term, sum N w k^p, N w sigma^p and N w over
 //     the bins with N > 0 and k > 0 (mean_spectrum.jl:43-82);
@@ -157,6 +159,147 @@ __global__ void __launch_bounds__(256) terms_kernel(const T* __restrict__ N, Ter
         }
 }
 
+// Two-kernel form for up to 4 terms. terms_cols_kernel (one warp per column): m0, the mean-spectrum
+// integrals and every term's per-cell values (x0, x1), written to tcol[c * n + t]. terms_bins_kernel:
+// one thread per (m, n) bin walking a chunk of columns with its bin's table entries in registers
+// (NT terms, unrolled), the column values read once per warp (all lanes read the same record) and the
+// rates stored coalesced along kappa. The per-bin arithmetic is terms_kernel's.
+template <typename T>
+__global__ void __launch_bounds__(256) terms_cols_kernel(const T* __restrict__ N, TermsArgs a, double2* __restrict__ tcol) {
+    const int64_t c = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (c >= a.P) return;  // uniform per warp
+    const int64_t Nk = a.Nk, Np = a.Np, nb = Nk * Np;
+    // the column pass: m0 and the integrals of the first mean-spectrum term together, four independent
+    // partial sums per lane (directions n mod 4) so the loads of four directions are in flight at once
+    int tm = -1;
+    for (int t = a.n - 1; t >= 0; --t)
+        if (a.kind[t] == RPL_TERM_MEAN_SPECTRUM) tm = t;
+    const double* tbm = a.tabs + (int64_t)(tm < 0 ? 0 : tm) * TABS * nb;
+    double m0p[4] = {0.0, 0.0, 0.0, 0.0}, skp[4] = {0.0, 0.0, 0.0, 0.0}, ssp[4] = {0.0, 0.0, 0.0, 0.0},
+           sdp[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int64_t m = lane; m < Nk; m += 32)
+        for (int64_t n0 = 0; n0 < Np; n0 += 4) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int64_t n = n0 + q;
+                if (n < Np) {
+                    const double v = (double)N[(n * a.P + c) * Nk + m];
+                    const int64_t b = m + Nk * n;
+                    m0p[q] += v * a.weights[b];
+                    if (tm >= 0 && v > 0.0) {
+                        skp[q] += v * tbm[nb + b];
+                        ssp[q] += v * tbm[2 * nb + b];
+                        sdp[q] += v * tbm[3 * nb + b];
+                    }
+                }
+            }
+        }
+    const double m0 = warp_sum((m0p[0] + m0p[1]) + (m0p[2] + m0p[3]));
+    for (int t = 0; t < a.n; ++t) {
+        const double rate = a.rate_field[t] ? a.rate_field[t][c] : a.rate[t];
+        double x0 = 0.0, x1 = 0.0;
+        switch (a.kind[t]) {
+            case RPL_TERM_EXPONENTIAL_WIND:
+                x0 = rate;
+                break;
+            case RPL_TERM_WAVE_AGE_WIND:
+                x0 = rate;
+                x1 = a.speed_field[t] ? a.speed_field[t][c] : a.speed[t];
+                break;
+            case RPL_TERM_WHITECAPPING: {
+                const double excess = fmax(m0 / a.p[t][0] - 1.0, 0.0);
+                x0 = rate * pow(excess, a.p[t][1]);
+                break;
+            }
+            default: {  // mean spectrum: x0 = -C_ds (m0 kbar^2)^2 sigmabar, x1 = kbar (0: no dissipation)
+                double sk, ss, sd;
+                if (t == tm) {
+                    sk = (skp[0] + skp[1]) + (skp[2] + skp[3]);
+                    ss = (ssp[0] + ssp[1]) + (ssp[2] + ssp[3]);
+                    sd = (sdp[0] + sdp[1]) + (sdp[2] + sdp[3]);
+                } else {   // a further mean-spectrum term: its own pass
+                    const double* tb = a.tabs + (int64_t)t * TABS * nb;
+                    sk = ss = sd = 0.0;
+                    for (int64_t n = 0; n < Np; ++n)
+                        for (int64_t m = lane; m < Nk; m += 32) {
+                            const double v = (double)N[(n * a.P + c) * Nk + m];
+                            const int64_t b = m + Nk * n;
+                            if (v > 0.0) {
+                                sk += v * tb[nb + b];
+                                ss += v * tb[2 * nb + b];
+                                sd += v * tb[3 * nb + b];
+                            }
+                        }
+                }
+                const double num_k = warp_sum(sk), num_s = warp_sum(ss), den = warp_sum(sd);
+                const double q = a.p[t][3];
+                const double kbar = den > 0.0 ? pow(num_k / den, 1.0 / q) : 0.0;
+                const double sbar = den > 0.0 ? pow(num_s / den, 1.0 / q) : 0.0;
+                if (m0 > 0.0 && kbar > 0.0) {
+                    const double alpha = m0 * kbar * kbar;
+                    x0 = -a.p[t][0] * alpha * alpha * sbar;
+                    x1 = kbar;
+                }
+                break;
+            }
+        }
+        if (lane == 0) tcol[c * a.n + t] = make_double2(x0, x1);
+    }
+}
+
+constexpr int TERM_COLS = 128;   // columns per thread in terms_bins_kernel (more on very large grids)
+
+template <typename T, int NT>
+__global__ void __launch_bounds__(256) terms_bins_kernel(TermsArgs a, const double2* __restrict__ tcol, T* __restrict__ R,
+                                                         int64_t chunk) {
+    const int64_t nb = a.Nk * a.Np;
+    const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb) return;
+    const int64_t Nk = a.Nk, m = b % Nk, n = b / Nk;
+    const int64_t c0 = (int64_t)blockIdx.y * chunk, c1 = min(c0 + chunk, a.P);
+    double t0[NT], t1[NT], t2[NT];
+#pragma unroll
+    for (int t = 0; t < NT; ++t) {
+        const double* tb = a.tabs + (int64_t)t * TABS * nb;
+        t0[t] = tb[b];
+        t1[t] = tb[nb + b];
+        t2[t] = tb[2 * nb + b];
+    }
+    for (int64_t c = c0; c < c1; ++c) {
+        double r = 0.0;
+#pragma unroll
+        for (int t = 0; t < NT; ++t) {
+            const double2 x = __ldg(tcol + c * NT + t);
+            switch (a.kind[t]) {
+                case RPL_TERM_EXPONENTIAL_WIND:
+                    r += x.x * t0[t];
+                    break;
+                case RPL_TERM_WAVE_AGE_WIND: {
+                    const double al = t0[t];
+                    if (al > 0.0) {
+                        const double excess = fmax(x.y * al * t1[t] - a.p[t][0], 0.0);
+                        r += x.x * pow_nonneg(excess, a.p[t][1]) * t2[t];
+                    }
+                    break;
+                }
+                case RPL_TERM_WHITECAPPING:
+                    r -= x.x * t0[t];
+                    break;
+                default: {
+                    const double k = t0[t];
+                    if (x.y > 0.0 && k > 0.0) {
+                        const double ratio = k / x.y;
+                        r -= x.x * (a.p[t][1] * ratio + a.p[t][2] * ratio * ratio);
+                    }
+                    break;
+                }
+            }
+        }
+        R[(n * a.P + c) * Nk + m] = (T)r;
+    }
+}
+
 // integral of max(cos, 0)^power over [a1, a2] (power >= 0 an integer): the antiderivative of cos^power
 // by its reduction formula, summed over the half periods where cos > 0
 double cos_power_antiderivative(double x, int power) {
@@ -227,9 +370,11 @@ std::string check_term(const rpl_source_term& t) {
 void free_terms(Handle* h) {
     if (h->d_lin_rates) cudaFree(h->d_lin_rates);
     if (h->d_terms) cudaFree(h->d_terms);
+    if (h->d_tcol) cudaFree(h->d_tcol);
     h->bytes -= h->terms_bytes;
     h->d_lin_rates = nullptr;
     h->d_terms = nullptr;
+    h->d_tcol = nullptr;
     h->terms_bytes = 0;
     h->n_terms = 0;
 }
@@ -253,7 +398,30 @@ cudaError_t launch_terms(const Handle& h, const void* Nin, cudaStream_t s) {
     a.tabs = h.d_terms;
     a.weights = h.d_weights;
     const unsigned blocks = (unsigned)((a.P * 32 + 255) / 256);
-    if (h.precision == RPL_FP64)
+    const bool fp64 = h.precision == RPL_FP64;
+    if (h.d_tcol) {   // up to 4 terms: column values, then the bins
+        if (fp64) terms_cols_kernel<double><<<blocks, 256, 0, s>>>((const double*)Nin, a, h.d_tcol);
+        else terms_cols_kernel<float><<<blocks, 256, 0, s>>>((const float*)Nin, a, h.d_tcol);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        const int64_t chunk = std::max<int64_t>(TERM_COLS, (a.P + 65534) / 65535);   // grid.y <= 65535
+        const dim3 grid((unsigned)((a.Nk * a.Np + 255) / 256), (unsigned)((a.P + chunk - 1) / chunk));
+        switch (a.n) {
+#define RPL_BINS(NT)                                                                                           \
+    case NT:                                                                                                   \
+        if (fp64) terms_bins_kernel<double, NT><<<grid, 256, 0, s>>>(a, h.d_tcol, (double*)h.d_lin_rates, chunk); \
+        else terms_bins_kernel<float, NT><<<grid, 256, 0, s>>>(a, h.d_tcol, (float*)h.d_lin_rates, chunk);  \
+        break;
+            RPL_BINS(1)
+            RPL_BINS(2)
+            RPL_BINS(3)
+            RPL_BINS(4)
+#undef RPL_BINS
+            default: return cudaErrorInvalidValue;
+        }
+        return cudaGetLastError();
+    }
+    if (fp64)
         terms_kernel<double><<<blocks, 256, 0, s>>>((const double*)Nin, a, (double*)h.d_lin_rates);
     else
         terms_kernel<float><<<blocks, 256, 0, s>>>((const float*)Nin, a, (float*)h.d_lin_rates);
@@ -354,12 +522,14 @@ extern "C" int rpl_set_source_terms(rpl_handle* hh, const rpl_source_term* terms
         }
     }
     const int64_t rate_bytes = h->units * (int64_t)h->elem, tab_bytes = (int64_t)host.size() * 8;
+    const int64_t col_bytes = count <= 4 ? P * count * (int64_t)sizeof(double2) : 0;
     const int64_t limit = d.memory_limit_bytes;
-    if (limit > 0 && h->bytes + rate_bytes + tab_bytes > limit)
-        return fail(RPL_ERR_OOM, "source terms need " + std::to_string(rate_bytes + tab_bytes) +
+    if (limit > 0 && h->bytes + rate_bytes + tab_bytes + col_bytes > limit)
+        return fail(RPL_ERR_OOM, "source terms need " + std::to_string(rate_bytes + tab_bytes + col_bytes) +
                                      " more device bytes, above the memory limit");
     e = cudaMalloc(&h->d_lin_rates, rate_bytes);
     if (e == cudaSuccess) e = cudaMalloc((void**)&h->d_terms, tab_bytes);
+    if (e == cudaSuccess && col_bytes) e = cudaMalloc((void**)&h->d_tcol, col_bytes);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(h->d_terms, host.data(), tab_bytes, cudaMemcpyHostToDevice, h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
@@ -368,7 +538,7 @@ extern "C" int rpl_set_source_terms(rpl_handle* hh, const rpl_source_term* terms
         return fail(e == cudaErrorMemoryAllocation ? RPL_ERR_OOM : RPL_ERR_CUDA,
                     std::string("rpl_set_source_terms: ") + cudaGetErrorString(e));
     }
-    h->terms_bytes = rate_bytes + tab_bytes;
+    h->terms_bytes = rate_bytes + tab_bytes + col_bytes;
     h->bytes += h->terms_bytes;
     for (int t = 0; t < count; ++t) {
         h->terms[t] = dev[t];

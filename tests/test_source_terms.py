@@ -176,6 +176,19 @@ def test_linear_terms_match_oracle(oracle_mod, precision, tol):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-12), ("fp32", 1e-5)])
+def test_five_terms_match_oracle(oracle_mod, precision, tol):
+    """More than four terms take the one-kernel form of the rates (one warp per column for both passes)."""
+    w = random_terms_workload(N=16, Nk=16, Np=24, seed=4)
+    w.sources = SourceTermSet(*w.sources.terms, ExponentialWindInput(rate=1e-5, direction=-1.2, spreading_power=4))
+    m = w.model(precision)
+    G = rp.interior(rp.compute_tendencies(m))
+    Go = oracle_mod.Oracle(w).tendency(w.N0)
+    assert np.linalg.norm(G - Go) <= tol * np.linalg.norm(Go)
+    m.close()
+
+
+@pytest.mark.gpu
 def test_reference_source_tests_on_gpu(oracle_mod):
     """The whitecapping ratio and the equilibrium tendency through the library (FP64)."""
     wc = WhitecappingDissipation(rate=0.2, saturation_threshold=0.1, saturation_power=1.0, wavenumber_power=2.0,
