@@ -98,7 +98,7 @@ WORKLOAD_NAMES = {"seamount": "seamount_eddies", "hurricane": "hurricane_swell",
                   "learned": "hurricane_swell (learned source)", "selfcoupled": "self_coupled_swell"}
 TRAFFIC_SUFFIX = {"seamount": "", "hurricane": "_hurricane", "selfcoupled": "_selfcoupled"}
 # the FP32 stage kernels each workload runs (refraction: two passes per stage; intrinsic: one fused kernel)
-STAGE_KERNELS = {"seamount": "xyw_kernel+kq_kernel", "hurricane": "tile_kernel",
+STAGE_KERNELS = {"seamount": "xyw_kernel+kq_kernel", "hurricane": "xyw_kernel+ks_kernel",
                  "selfcoupled": "xyw_kernel+kq_kernel"}
 DATA = {"seamount": "synthetic (seeded seamount depth, eddy currents, JONSWAP-like N0)",
         "hurricane": "synthetic (Holland hurricane on a linear track, uniform N0 = 1e-6)",
@@ -122,13 +122,14 @@ def make_workload(name, n, nsteps, n0_dtype=np.float64):
 
 
 def launches_per_step(name, precision="fp32"):
-    """Our kernels per RK3 step. A refraction stage is two launches in FP32 (x/y flux pass, then the
-    kappa/phi pass with the stage update) and one fused launch in FP64; the hurricane (intrinsic
-    transport, one fused launch per stage) adds 1 wind + 3 stress-cap kernels; the self-coupled swell
-    adds 2 coupling kernels per stage, and in FP32 the refresh of the velocity planes of the x/y pass."""
+    """Our kernels per RK3 step. A stage is two launches in FP32 (refraction: the x/y flux pass, then the
+    kappa/phi pass with the stage update; the hurricane's intrinsic transport with the bundle sources: the
+    x/y pass, then the sources and the update) and one fused launch in FP64; the hurricane adds 1 wind + 3
+    stress-cap kernels; the self-coupled swell adds 2 coupling kernels per stage, and in FP32 the refresh
+    of the velocity planes of the x/y pass."""
     per_stage = 2 if precision == "fp32" else 1
     coupling = 3 if precision == "fp32" else 2
-    return {"seamount": 3 * per_stage, "selfcoupled": 3 * (per_stage + coupling)}.get(name, 7)
+    return {"seamount": 3 * per_stage, "selfcoupled": 3 * (per_stage + coupling)}.get(name, 3 * per_stage + 4)
 
 
 def current_launches(precision):

@@ -263,7 +263,7 @@ int rpl_create(const rpl_desc* d, rpl_handle** out) {
     int64_t need = 3 * units * (int64_t)elem + 16 * c3 * 8 + (d->depth_kind == RPL_DEPTH_FIELD ? (c3 + P) * 8 : 0) +
                    (4 * P + 2 * (d->Nx + d->Ny)) * 8 + 6 * P * 8 + 8 * nb * 8 +
                    (d->precision == RPL_FP32 && d->transport == RPL_TRANSPORT_REFRACTION ? units * 4 + 3 * c3 * 4 : 0) +
-                   (d->precision == RPL_FP32 && d->transport == RPL_TRANSPORT_INTRINSIC ? c3 * 4 : 0);
+                   (d->precision == RPL_FP32 && d->transport == RPL_TRANSPORT_INTRINSIC ? c3 * 4 + units * 4 : 0);
     if (d->memory_limit_bytes > 0 && need > d->memory_limit_bytes)
         return fail(RPL_ERR_OOM, "model needs " + std::to_string(need) + " device bytes, above the memory limit of " +
                                      std::to_string(d->memory_limit_bytes));
@@ -404,7 +404,10 @@ int rpl_create(const rpl_desc* d, rpl_handle** out) {
                              !h->force_column_kernel;
     if ((h->d_sxy || intrinsic32) && rpl::xyw_supported(*h) && !h->pass_a_tiles) {
         // the y-walk x/y kernels: FP32 velocity planes (intrinsic: c_g only) and upwind ratios
-        TRY(dalloc(h, &h->d_vel32, (h->d_sxy ? 3 : 1) * c3));
+        const bool refract_planes = h->d_sxy != nullptr;
+        TRY(dalloc(h, &h->d_vel32, (refract_planes ? 3 : 1) * c3));
+        // intrinsic stages with the bundle or learned sources run the x/y pass, then the sources: S
+        if (!refract_planes) TRY(dalloc(h, &h->d_sxy, units));
         h->vel_regions = rpl::xyw_regions(*h);
         TRY(dalloc(h, &h->d_rmax, 2 * h->vel_regions * d->Nk));
     }

@@ -277,6 +277,8 @@ int64_t xyw_regions(const Handle& h);             // regions of the upwind ratio
 // d_vel32).
 cudaError_t launch_vel32(const Handle& h, cudaStream_t s);
 cudaError_t launch_xyw(const TileArgs& a, cudaStream_t s);   // writes a.sxy for rows [j_lo, j_hi)
+// The same x/y pass for intrinsic transport (no currents): S = fx + fy into a.sxy.
+cudaError_t launch_xy_intrinsic(const TileArgs& a, cudaStream_t s);
 // The whole stage of intrinsic transport (no currents) without sources (src 0) or with the SourceTermSet
 // rates (src 3, the tile body's SRC).
 cudaError_t launch_xyi(const TileArgs& a, int src, cudaStream_t s);

@@ -760,6 +760,67 @@ __global__ void __launch_bounds__(CPB * L, MINB) kq_kernel(const TileArgs p) {
     }
 }
 
+// Second pass of an intrinsic stage with the bundle (SRC 1) or the learned (SRC 2) sources, after the
+// y-walk x/y pass stored S = fx + fy: one thread per (cell, kappa pair) walking the phi ring with the
+// cell's wind constants and its bins' constants loaded once; G = -S, the sources and the stage update
+// as the tile body (G = -(fx + fy) there).
+template <int L, int CPB, int MINB, int SRC>
+__global__ void __launch_bounds__(CPB * L, MINB) ks_kernel(const TileArgs p) {
+    static_assert(SRC == 1 || SRC == 2, "bundle or learned sources");
+    const float* __restrict__ S = p.sxy;
+    const float* __restrict__ Nin = p.Nin;
+    const float* N0 = p.N0;
+    float* Nout = p.Nout;
+    const int Nx = p.Nx, Ny = p.Ny, Nk = p.Nk, Np = p.Np;
+    const int64_t slice = (int64_t)Nx * Ny * Nk;
+    const int64_t P = (int64_t)Nx * (p.j_hi - p.j_lo);
+    const int tid = threadIdx.x, l = tid % L;
+    const int64_t cidx = (int64_t)blockIdx.x * CPB + tid / L;
+    const bool live_cell = cidx < P;
+    const int64_t cc = (live_cell ? cidx : P - 1) + (int64_t)Nx * p.j_lo;
+    const int m0 = 2 * l;
+    const bool live = live_cell && m0 < Nk;
+    const int mc = m0 < Nk ? m0 : Nk - 2;
+    const int64_t home = cc * Nk + mc;
+    const Cell32 wc = load_cell32(p.cell32 + 8 * cc);
+    const Bin32 wb0 = load_bin32(p.bin32 + 8 * mc), wb1 = load_bin32(p.bin32 + 8 * (mc + 1));
+    bool plain_src = SRC == 1;
+    const float* lrow = nullptr;
+    if constexpr (SRC == 2) {
+        plain_src = __ldg(p.lflag + cc) != 0u;
+        lrow = p.lrate + cc * ((int64_t)Nk * Np) + mc;
+    }
+    const float dt = p.dt, ca = p.a, cb = p.b;
+    for (int n = 0; n < Np; ++n) {
+        const int64_t off = slice * n + home;
+        const float2 c = *reinterpret_cast<const float2*>(Nin + off);
+        const float2 sxy = *reinterpret_cast<const float2*>(S + off);
+        const float2 n0v = (p.stage == 1 || !live) ? f2(0.f) : *reinterpret_cast<const float2*>(N0 + off);
+        float2 G = mul2(f2(-1.f), sxy);
+        if (plain_src) {
+            const float2 cs = __ldg(p.cs32 + n);
+            G.x += source32(p, wc, wb0, cs.x, cs.y, c.x);
+            G.y += source32(p, wc, wb1, cs.x, cs.y, c.y);
+        } else if constexpr (SRC == 2) {  // learned: N * rate, rate = lscale * sinh(network output of bin (m, n))
+            const float2 y = __ldg(reinterpret_cast<const float2*>(lrow + (int64_t)n * Nk));
+            G = fma2(mul2(c, f2(p.lscale)), make_float2(sinhf(y.x), sinhf(y.y)), G);
+        }
+        float2 st = fma2(f2(dt), G, c);
+        st.x = relu(st.x);
+        st.y = relu(st.y);
+        float2 out = st;
+        if (p.stage != 1) {
+            out = fma2(f2(ca), n0v, mul2(f2(cb), st));
+            out.x = relu(out.x);
+            out.y = relu(out.y);
+        }
+        if (live) {
+            if (!isfinite(out.x) || !isfinite(out.y)) atomicOr(p.err, 1u);
+            *reinterpret_cast<float2*>(Nout + off) = out;
+        }
+    }
+}
+
 // Single-model kernel: one CTA per TX x TY tile, MINB CTAs resident per SM.
 template <int L, int TX, int TY, int MINB, bool REFRACT, int SRC>
 __global__ void __launch_bounds__(TX * TY * L, MINB) tile_kernel(const TileArgs p) {
@@ -870,8 +931,20 @@ cudaError_t launch_L(const Handle& h, const StageParams& p, const TileArgs& a, c
         if (src == 2) return launch_variant<L, true, 2>(a, tiles, s);
         return src ? launch_variant<L, true, 1>(a, tiles, s) : launch_variant<L, true, 0>(a, tiles, s);
     }
-    // the y-walk form (rpl_xyw.cu, one reconstruction per face) without the bundle or learned sources
+    // the y-walk form (rpl_xyw.cu, one reconstruction per face): one pass without the bundle or learned
+    // sources; with them the x/y pass stores S and ks_kernel adds the sources per cell (their per-cell
+    // constants loaded once per phi ring) and updates
     if (a.rmax && (src == 0 || src == 3)) return launch_xyi(a, src, s);
+    if (a.rmax && a.sxy && (src == 1 || src == 2)) {
+        cudaError_t e = launch_xy_intrinsic(a, s);
+        if (e != cudaSuccess) return e;
+        constexpr int CPB = 256 / L;
+        const int64_t cells = (int64_t)a.Nx * (a.j_hi - a.j_lo);
+        const unsigned blocks = (unsigned)((cells + CPB - 1) / CPB);
+        if (src == 1) ks_kernel<L, CPB, 2, 1><<<blocks, CPB * L, 0, s>>>(a);
+        else ks_kernel<L, CPB, 2, 2><<<blocks, CPB * L, 0, s>>>(a);
+        return cudaGetLastError();
+    }
     if (src == 3) return launch_variant<L, false, 3>(a, tiles, s);
     if (src == 2) return launch_variant<L, false, 2>(a, tiles, s);
     return src ? launch_variant<L, false, 1>(a, tiles, s) : launch_variant<L, false, 0>(a, tiles, s);

@@ -63,10 +63,13 @@ struct Lay {
 // FSRC 3 the SourceTermSet rates, and the stage update, written to Nout. (The bundle and the learned
 // sources stay in the tile kernel, which walks the phi ring at a fixed cell and loads their per-cell
 // constants once: measured on the 768^2 hurricane, 24.4 against 30.3 ms per step.)
+// FSRC -2: pass A of an intrinsic stage with the bundle or learned sources (no currents, S stored; the
+// sources and the update follow in ks_kernel, rpl_tile32.cu).
 template <int L, int XM, int YM, int FSRC>
 __device__ __forceinline__ void xyw_body(const TileArgs& p, float* smem, int n, int tx, int js, int je) {
-    static_assert(FSRC == -1 || FSRC == 0 || FSRC == 3, "pass A, or an intrinsic stage without bundle sources");
-    constexpr bool FUSED = FSRC >= 0;
+    static_assert(FSRC == -2 || FSRC == -1 || FSRC == 0 || FSRC == 3,
+                  "pass A, or an intrinsic stage without bundle sources");
+    constexpr bool FUSED = FSRC >= 0, CURR = FSRC == -1;   // CURR: currents (refraction)
     using Y = Lay<L>;
     constexpr int CX = Y::CX, KP = Y::KP, ROW = Y::ROW;
     const int Nx = p.Nx, Ny = p.Ny, Nk = p.Nk;
@@ -112,7 +115,7 @@ __device__ __forceinline__ void xyw_body(const TileArgs& p, float* smem, int n, 
     Q vx, vy, vc = {f2(1.f), f2(1.f)};
     auto vload = [&](int r) {
         const int e = r * rs + colm;
-        if constexpr (!FUSED) {
+        if constexpr (CURR) {
             vx = ldgq(p.ux32 + e);
             vy = ldgq(p.uy32 + e);
         }
@@ -126,7 +129,7 @@ __device__ __forceinline__ void xyw_body(const TileArgs& p, float* smem, int n, 
             ux = qmul(vc, ux);
             uy = qmul(vc, uy);
         }
-        if constexpr (!FUSED) {
+        if constexpr (CURR) {
             ux = qadd(ux, vx);
             uy = qadd(uy, vy);
         }
@@ -318,16 +321,14 @@ __global__ void __launch_bounds__(XTHREADS, 2) xyw_kernel(const TileArgs p, int 
     const int allyp = __syncthreads_and(!live || (cy && yp)), allyn = __syncthreads_and(!live || (cy && yn));
     const int xm = allxp ? POS : (allxn ? NEG : MIX);
     const int ym = allyp ? POS : (allyn ? NEG : MIX);
-    switch (xm * 3 + ym) {
-        case 0: xyw_body<L, POS, POS, FSRC>(p, smem, n, tx, js, je); break;
-        case 1: xyw_body<L, POS, NEG, FSRC>(p, smem, n, tx, js, je); break;
-        case 2: xyw_body<L, POS, MIX, FSRC>(p, smem, n, tx, js, je); break;
-        case 3: xyw_body<L, NEG, POS, FSRC>(p, smem, n, tx, js, je); break;
-        case 4: xyw_body<L, NEG, NEG, FSRC>(p, smem, n, tx, js, je); break;
-        case 5: xyw_body<L, NEG, MIX, FSRC>(p, smem, n, tx, js, je); break;
-        case 6: xyw_body<L, MIX, POS, FSRC>(p, smem, n, tx, js, je); break;
-        case 7: xyw_body<L, MIX, NEG, FSRC>(p, smem, n, tx, js, je); break;
-        default: xyw_body<L, MIX, MIX, FSRC>(p, smem, n, tx, js, je); break;
+    // the four sign-uniform bodies, else the general one (either axis mixed: 2-5% of the CTAs)
+    if (xm == MIX || ym == MIX) xyw_body<L, MIX, MIX, FSRC>(p, smem, n, tx, js, je);
+    else if (xm == POS) {
+        if (ym == POS) xyw_body<L, POS, POS, FSRC>(p, smem, n, tx, js, je);
+        else xyw_body<L, POS, NEG, FSRC>(p, smem, n, tx, js, je);
+    } else {
+        if (ym == POS) xyw_body<L, NEG, POS, FSRC>(p, smem, n, tx, js, je);
+        else xyw_body<L, NEG, NEG, FSRC>(p, smem, n, tx, js, je);
     }
 }
 
@@ -422,6 +423,8 @@ cudaError_t launch_lanes(const TileArgs& a, cudaStream_t s) {
 }
 
 cudaError_t launch_xyw(const TileArgs& a, cudaStream_t s) { return launch_lanes<-1>(a, s); }
+
+cudaError_t launch_xy_intrinsic(const TileArgs& a, cudaStream_t s) { return launch_lanes<-2>(a, s); }
 
 cudaError_t launch_xyi(const TileArgs& a, int src, cudaStream_t s) {
     if (src != 0 && src != 3) return cudaErrorInvalidValue;
